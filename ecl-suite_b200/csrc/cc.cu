@@ -1,0 +1,239 @@
+// Connected components (ECL-CC contract).
+//
+// Result contract (src/racefree/egr-input/CC/ECL-CC-atomic.cu): every vertex v
+// hooks only along its list entries u = nlist[i] with u < v (:132, :174,
+// :218), roots are always hooked larger -> smaller (:139-146) and flatten
+// points each vertex at its root (:250-264).  Hence the label of v is the
+// smallest vertex id of v's component in the graph whose edges are
+// {(v, u) : u in list(v), u < v}.  That value does not depend on the schedule,
+// so any union-find with the same hooking rule reproduces it bit for bit.
+//
+// B200 design:
+//  * cc_init   - parent[v] = first smaller neighbour (one free hook per vertex).
+//  * cc_hook   - one pass over the vertices, 32 per warp.  Lists of <= 16
+//                entries are walked by their own lane; lists of up to
+//                kChunk entries are walked by the whole warp (ballot loop,
+//                coalesced 128-byte nlist reads); longer lists are cut into
+//                kChunk-entry chunk records for cc_chunks.
+//  * cc_chunks - warp per chunk record, so a 163k-entry R-MAT hub is spread
+//                over ~160 warps instead of serialising one block.
+//  * cc_flatten- label[v] = root(v).
+// The parent array IS the output label array (no extra n-sized buffer).
+// All parent accesses are device-scope relaxed atomics; links use CAS.
+#include "runtime.cuh"
+
+namespace ecl {
+namespace {
+
+using namespace dev;
+
+constexpr int kTPB = 256;
+constexpr int kLaneMax = 16;   // lists up to this length: lane-level
+constexpr int kChunk = 2048;   // lists longer than this: chunk records
+
+// Row [beg, end) of v, or empty when the row is malformed (cc_init reports it).
+__device__ __forceinline__ void cc_row(const int* nindex, int v, int m, int& beg, int& end) {
+  beg = __ldg(&nindex[v]);
+  end = __ldg(&nindex[v + 1]);
+  if (beg < 0 || end < beg || end > m) beg = end = 0;
+}
+
+// Entries outside [0, n) raise ECL_ERR_BAD_GRAPH and are skipped.
+__device__ __forceinline__ bool cc_valid(int u, int n, Status* status) {
+  if ((unsigned)u < (unsigned)n) return true;
+  raise(status, ECL_ERR_BAD_GRAPH, u);
+  return false;
+}
+
+struct CCCounters {
+  int nchunks;
+  int pad[63];
+};
+
+// Root of v with path splitting.  Parent pointers only ever point at
+// smaller ids, so a vertex is a root iff parent[v] == v.
+__device__ __forceinline__ int cc_root(int v, int* parent) {
+  int cur = ld(&parent[v]);
+  if (cur == v) return v;
+  int prev = v;
+  int next;
+  while (cur > (next = ld(&parent[cur]))) {
+    st(&parent[prev], next);
+    prev = cur;
+    cur = next;
+  }
+  return cur;
+}
+
+// Links the trees rooted (as last seen) at a and b; returns the root that
+// survived the link as last seen by this thread.
+__device__ __forceinline__ int cc_link(int a, int b, int* parent) {
+  while (a != b) {
+    if (a < b) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    const int seen = cas(&parent[a], a, b);
+    if (seen == a) return b;
+    a = cc_root(seen, parent);
+    b = cc_root(b, parent);
+  }
+  return a;
+}
+
+// Also checks the CSR rows once: a malformed row (end < beg, or outside
+// [0, m]) raises ECL_ERR_BAD_GRAPH and is treated as empty by every kernel.
+__global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restrict__ nindex,
+                                                const int* __restrict__ nlist, int* __restrict__ parent,
+                                                Status* __restrict__ status) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
+    if (beg < 0 || end < beg || end > m) {
+      raise(status, ECL_ERR_BAD_GRAPH, v);
+      beg = end = 0;
+    }
+    int p = v;
+    for (int i = beg; i < end; i++) {
+      const int u = __ldg(&nlist[i]);
+      if (u < v && u >= 0) {
+        p = u;
+        break;
+      }
+    }
+    parent[v] = p;
+  }
+}
+
+__global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restrict__ nindex,
+                                                const int* __restrict__ nlist, int* __restrict__ parent,
+                                                int2* __restrict__ chunks, CCCounters* __restrict__ ctr,
+                                                Status* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  for (int base = warp * 32; base < n; base += nwarps * 32) {
+    const int v = base + lane;
+    int beg = 0, end = 0;
+    if (v < n) cc_row(nindex, v, m, beg, end);
+    const int deg = end - beg;
+    if (deg > kChunk) {
+      const int nc = (deg + kChunk - 1) / kChunk;
+      const int at = fetch_add(&ctr->nchunks, nc);
+      for (int c = 0; c < nc; c++) chunks[at + c] = make_int2(v, beg + c * kChunk);
+    } else if (deg > 0 && deg <= kLaneMax) {
+      int rv = -1;
+      for (int i = beg; i < end; i++) {
+        const int u = __ldg(&nlist[i]);
+        if (u < v && cc_valid(u, n, status)) {
+          if (rv < 0) rv = cc_root(v, parent);
+          const int ru = cc_root(u, parent);
+          if (ru != rv) rv = cc_link(rv, ru, parent);
+        }
+      }
+    }
+    // Medium lists: the whole warp walks one list at a time.
+    unsigned mid = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
+    while (mid) {
+      const int who = __ffs(mid) - 1;
+      mid &= mid - 1;
+      const int wv = __shfl_sync(kFull, v, who);
+      const int wbeg = __shfl_sync(kFull, beg, who);
+      const int wend = __shfl_sync(kFull, end, who);
+      int rv = -1;
+      for (int i = wbeg + lane; i < wend; i += 32) {
+        const int u = __ldg(&nlist[i]);
+        if (u < wv && cc_valid(u, n, status)) {
+          if (rv < 0) rv = cc_root(wv, parent);
+          const int ru = cc_root(u, parent);
+          if (ru != rv) rv = cc_link(rv, ru, parent);
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTPB) cc_chunks(int n, const int* __restrict__ nindex,
+                                                  const int* __restrict__ nlist, int* __restrict__ parent,
+                                                  const int2* __restrict__ chunks, const CCCounters* __restrict__ ctr,
+                                                  Status* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  const int total = ctr->nchunks;
+  for (int c = warp; c < total; c += nwarps) {
+    const int2 rec = chunks[c];
+    const int v = rec.x;
+    const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
+    int rv = -1;
+    for (int i = rec.y + lane; i < end; i += 32) {
+      const int u = __ldg(&nlist[i]);
+      if (u < v && cc_valid(u, n, status)) {
+        if (rv < 0) rv = cc_root(v, parent);
+        const int ru = cc_root(u, parent);
+        if (ru != rv) rv = cc_link(rv, ru, parent);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTPB) cc_flatten(int n, int* __restrict__ parent) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    int cur = ld(&parent[v]);
+    const int first = cur;
+    int next;
+    while (cur > (next = ld(&parent[cur]))) cur = next;
+    if (cur != first) st(&parent[v], cur);
+  }
+}
+
+void cc_layout(Carve& c, int n, int m, CCCounters** ctr, int2** chunks) {
+  (void)n;
+  *ctr = c.take<CCCounters>(1);
+  *chunks = c.take<int2>((size_t)(2 * (m / kChunk) + 2));
+}
+
+}  // namespace
+
+size_t cc_workspace_bytes(int n, int m) {
+  Carve c;
+  CCCounters* ctr;
+  int2* chunks;
+  cc_layout(c, n, m, &ctr, &chunks);
+  return c.bytes();
+}
+
+}  // namespace ecl
+
+extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* opts) {
+  using namespace ecl;
+  ecl_opts local{};
+  if (!opts) opts = &local;
+  if (!label) return ECL_ERR_INVALID_ARG;
+  Solve s(g, opts);
+  ecl_status st = s.begin(GraphNeeds{}, g ? cc_workspace_bytes(g->nodes, g->edges) : 0);
+  if (st != ECL_OK) return s.finish(st);
+  int* parent = s.output(label, (size_t)s.n);
+  if (!parent) return s.finish(ECL_ERR_OOM);
+  Carve c{s.ws};
+  CCCounters* ctr;
+  int2* chunks;
+  cc_layout(c, s.n, s.m, &ctr, &chunks);
+  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
+
+  s.start_timer();
+  if (cudaMemsetAsync(ctr, 0, sizeof(CCCounters), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
+  ECL_LAUNCH(cc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, s.status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, chunks, ctr, s.status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, parent, chunks, ctr, s.status);
+  ECL_LAUNCH(cc_flatten, grid, kTPB, 0, s.stream, s.n, parent);
+  s.stop_timer();
+  return s.finish();
+}
+
+extern "C" ecl_status ecl_compute_cc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,
+                                     int32_t* nstat) {
+  ecl_graph_view g{nodes, edges, nidx, nlist, nullptr, ECL_HOST, 0};
+  ecl_opts o{};
+  return ecl_cc(&g, nstat, &o);
+}

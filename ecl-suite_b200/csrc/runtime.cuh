@@ -1,0 +1,131 @@
+// Host runtime shared by the solver entry points: argument checks, staging of
+// host-resident CSR arrays, workspace carving, launch accounting, timing and
+// the read-back of the device status word.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+#include "ecl_b200.h"
+
+namespace ecl {
+
+// Process-wide count of kernel launches made by this library.
+extern std::atomic<uint64_t> g_launches;
+inline void count_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+// Records a CUDA failure message for ecl_last_error().
+void set_last_error(const char* where, cudaError_t e);
+void set_last_error_msg(const char* msg);
+
+#define ECL_CUDA_TRY(call)                          \
+  do {                                              \
+    cudaError_t ecl_e_ = (call);                    \
+    if (ecl_e_ != cudaSuccess) {                    \
+      ::ecl::set_last_error(#call, ecl_e_);         \
+      return ECL_ERR_CUDA;                          \
+    }                                               \
+  } while (0)
+
+// Launch + accounting.  Kernel launch errors surface at the next CUDA call.
+#define ECL_LAUNCH(kernel, grid, block, smem, stream, ...)        \
+  do {                                                            \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);   \
+    ::ecl::count_launch();                                        \
+  } while (0)
+
+struct DeviceInfo {
+  int device = -1;
+  int sms = 0;
+  int max_threads_per_sm = 0;
+  int major = 0, minor = 0;
+  size_t smem_optin = 0;
+};
+// Properties of the current device (cached per device id).
+ecl_status current_device(DeviceInfo* info);
+
+// Workspace carving: the same sequence of take() calls sizes a workspace
+// (base == nullptr) and then hands out 256-byte-aligned sub-buffers.
+struct Carve {
+  char* base = nullptr;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+  size_t bytes() const { return (off + 255) & ~size_t(255); }
+};
+
+// Requirements a solver places on its input graph.
+struct GraphNeeds {
+  bool weights = false;      // eweight must be non-NULL
+  bool symmetric = false;    // checked only when opts->validate
+  bool no_self_loops = false;  // checked only when opts->validate
+};
+
+// One solve: stages inputs/outputs and owns temporaries until finish().
+class Solve {
+ public:
+  Solve(const ecl_graph_view* g, ecl_opts* opts) : g_(g), opts_(opts) {}
+  ~Solve();
+
+  // Checks arguments, validates (if asked), stages the CSR on the device and
+  // provides `ws_bytes` of workspace.  The device Status block is placed at
+  // the start of the workspace and zeroed.
+  ecl_status begin(const GraphNeeds& needs, size_t ws_bytes);
+
+  // Device pointer through which the solver writes an output of `count`
+  // elements: the caller's pointer for device-resident graphs, else a
+  // temporary that finish() copies back to `user`.
+  template <class T>
+  T* output(T* user, size_t count) {
+    return static_cast<T*>(output_bytes(user, count * sizeof(T)));
+  }
+  void* output_bytes(void* user, size_t bytes);
+  // Device scratch outside the workspace (freed by finish()).
+  void* temp(size_t bytes);
+
+  void start_timer();
+  void stop_timer();
+  // Copies outputs back, synchronises, folds the device status into the
+  // return code and releases temporaries.
+  ecl_status finish(ecl_status st = ECL_OK);
+
+  int n = 0, m = 0;
+  const int* nindex = nullptr;
+  const int* nlist = nullptr;
+  const int* eweight = nullptr;
+  cudaStream_t stream = nullptr;
+  char* ws = nullptr;            // workspace base (Status block first)
+  size_t ws_size = 0;
+  dev::Status* status = nullptr;
+  DeviceInfo dev;
+  bool alloc_failed = false;
+
+ private:
+  const ecl_graph_view* g_;
+  ecl_opts* opts_;
+  struct Copy {
+    void* host;
+    void* dev;
+    size_t bytes;
+  };
+  std::vector<Copy> outs_;
+  std::vector<void*> temps_;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  bool timed_ = false;
+  bool finished_ = false;
+};
+
+// Offset of the first usable byte of a workspace after the Status block.
+constexpr size_t kStatusBytes = 256;
+
+}  // namespace ecl

@@ -1,0 +1,362 @@
+"""Python host binding of libeclb200.so (the B200-native race-free graph codes).
+
+The library is C++/CUDA behind a C ABI (include/ecl_b200.h); this module only
+marshals arguments through ctypes.  There is no Python or CPU compute path:
+if the shared library is missing the import fails, and every solver runs the
+sm_100a kernels.
+
+Operators mirror the reference's per-code contracts (ECL-Suite,
+src/racefree/...): ``cc`` returns nstat labels, ``mis`` the 0xfe/0 status
+bytes, ``gc`` colours, ``mst`` the in_mst edge flags, ``scc`` max-id labels,
+``apsp`` the distance matrix.  Arguments are either an :class:`Graph` of host
+numpy arrays (the call copies to the device and back) or a
+:class:`DeviceGraph` of torch CUDA tensors (nothing crosses PCIe).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libeclb200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"libeclb200.so not built at {LIB_PATH}; run `make -C ecl-suite_b200` or __graft_entry__.build()")
+
+lib = C.CDLL(LIB_PATH)
+
+# ---- status / enums --------------------------------------------------------------
+
+OK, ERR_INVALID_ARG, ERR_BAD_GRAPH, ERR_OOM, ERR_NO_CONVERGENCE, ERR_CUDA, ERR_IO, ERR_UNSUPPORTED, ERR_NO_DEVICE = range(9)
+HOST, DEVICE = 0, 1
+GRAPH_SYMMETRIC = 0x1
+CC, MIS, GC, MST, SCC, APSP = range(6)
+MIS_IN, MIS_OUT = 0xFE, 0x00
+APSP_INF = 0x7FFFFFFF // 2
+
+
+class EclError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        msg = lib.ecl_status_string(status).decode()
+        last = lib.ecl_last_error().decode()
+        super().__init__(f"{where}: {msg} ({status}){' - ' + last if last else ''}")
+        self.status = status
+
+
+class GraphView(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_int32),
+        ("edges", C.c_int32),
+        ("nindex", C.c_void_p),
+        ("nlist", C.c_void_p),
+        ("eweight", C.c_void_p),
+        ("location", C.c_int32),
+        ("flags", C.c_int32),
+    ]
+
+
+class Opts(C.Structure):
+    _fields_ = [
+        ("stream", C.c_void_p),
+        ("workspace", C.c_void_p),
+        ("workspace_bytes", C.c_size_t),
+        ("validate", C.c_int32),
+        ("max_rounds", C.c_int32),
+        ("elapsed_ms", C.c_float),
+        ("rounds", C.c_int32),
+    ]
+
+
+class CGraph(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_int32),
+        ("edges", C.c_int32),
+        ("nindex", C.POINTER(C.c_int32)),
+        ("nlist", C.POINTER(C.c_int32)),
+        ("eweight", C.POINTER(C.c_int32)),
+    ]
+
+
+_VP, _I32, _U64, _F64 = C.c_void_p, C.c_int32, C.c_uint64, C.c_double
+_PV, _PO, _PG = C.POINTER(GraphView), C.POINTER(Opts), C.POINTER(CGraph)
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+_sig("ecl_abi_version", C.c_int32, [])
+_sig("ecl_status_string", C.c_char_p, [C.c_int])
+_sig("ecl_last_error", C.c_char_p, [])
+_sig("ecl_workspace_bytes", C.c_size_t, [C.c_int, _I32, _I32])
+_sig("ecl_kernel_launches", C.c_uint64, [])
+_sig("ecl_cc", C.c_int, [_PV, _VP, _PO])
+_sig("ecl_mis", C.c_int, [_PV, _VP, _PO])
+_sig("ecl_gc", C.c_int, [_PV, _VP, _PO])
+_sig("ecl_mst", C.c_int, [_PV, _VP, C.POINTER(C.c_uint64), _PO])
+_sig("ecl_scc", C.c_int, [_PV, _VP, _PO])
+_sig("ecl_apsp", C.c_int, [_PV, _VP, C.c_int64, _PO])
+_sig("ecl_graph_read", C.c_int, [C.c_char_p, _PG])
+_sig("ecl_graph_write", C.c_int, [C.c_char_p, _PG])
+_sig("ecl_graph_free", None, [_PG])
+_sig("ecl_graph_validate", C.c_int, [_PV, _I32, _I32])
+_sig("ecl_gen_rmat", C.c_int, [_I32, _I32, _F64, _F64, _F64, _U64, _I32, _U64, _I32, _PG])
+_sig("ecl_gen_grid", C.c_int, [_I32, _I32, _F64, _U64, _U64, _I32, _PG])
+_sig("ecl_gen_er", C.c_int, [_I32, _F64, _U64, _I32, _U64, _I32, _I32, _PG])
+
+# Every symbol that include/ecl_b200.h declares (checked by the CPU tests).
+EXPORTED = [
+    "ecl_abi_version", "ecl_status_string", "ecl_last_error", "ecl_workspace_bytes", "ecl_kernel_launches",
+    "ecl_cc", "ecl_mis", "ecl_gc", "ecl_mst", "ecl_scc", "ecl_apsp",
+    "ecl_compute_cc", "ecl_compute_mis", "ecl_compute_gc", "ecl_compute_mst", "ecl_compute_scc", "ecl_compute_apsp",
+    "ecl_graph_read", "ecl_graph_write", "ecl_graph_free", "ecl_graph_validate",
+    "ecl_gen_rmat", "ecl_gen_grid", "ecl_gen_er",
+]
+
+
+def _check(st: int, where: str) -> None:
+    if st != OK:
+        raise EclError(st, where)
+
+
+# ---- graphs ----------------------------------------------------------------------
+
+
+@dataclass
+class Graph:
+    """ECLgraph CSR in host memory (library/ECLgraph.h:41-47)."""
+
+    nindex: np.ndarray
+    nlist: np.ndarray
+    eweight: Optional[np.ndarray] = None
+    symmetric: bool = False
+
+    def __post_init__(self):
+        self.nindex = np.ascontiguousarray(self.nindex, dtype=np.int32)
+        self.nlist = np.ascontiguousarray(self.nlist, dtype=np.int32)
+        if self.eweight is not None:
+            self.eweight = np.ascontiguousarray(self.eweight, dtype=np.int32)
+
+    @property
+    def nodes(self) -> int:
+        return int(self.nindex.shape[0] - 1)
+
+    @property
+    def edges(self) -> int:
+        return int(self.nlist.shape[0])
+
+    def view(self) -> GraphView:
+        v = GraphView()
+        v.nodes, v.edges = self.nodes, self.edges
+        v.nindex = self.nindex.ctypes.data
+        v.nlist = self.nlist.ctypes.data if self.edges else None
+        v.eweight = self.eweight.ctypes.data if self.eweight is not None else None
+        v.location = HOST
+        v.flags = GRAPH_SYMMETRIC if self.symmetric else 0
+        return v
+
+    def validate(self, symmetric: bool = False, no_self_loops: bool = False) -> bool:
+        v = self.view()
+        return lib.ecl_graph_validate(C.byref(v), int(symmetric), int(no_self_loops)) == OK
+
+    def write(self, path: str) -> None:
+        cg = CGraph(self.nodes, self.edges,
+                    self.nindex.ctypes.data_as(C.POINTER(C.c_int32)),
+                    self.nlist.ctypes.data_as(C.POINTER(C.c_int32)),
+                    self.eweight.ctypes.data_as(C.POINTER(C.c_int32)) if self.eweight is not None else None)
+        _check(lib.ecl_graph_write(path.encode(), C.byref(cg)), "ecl_graph_write")
+
+    def to_device(self, device: str = "cuda"):
+        import torch
+
+        return DeviceGraph(
+            torch.from_numpy(self.nindex).to(device),
+            torch.from_numpy(self.nlist).to(device) if self.edges else torch.zeros(1, dtype=torch.int32, device=device),
+            torch.from_numpy(self.eweight).to(device) if self.eweight is not None else None,
+            self.symmetric,
+            self.edges,
+        )
+
+
+def _take(cg: CGraph, symmetric: bool) -> Graph:
+    """Copies a library-allocated ecl_graph into numpy arrays and frees it."""
+    n, m = cg.nodes, cg.edges
+    try:
+        nindex = np.ctypeslib.as_array(cg.nindex, shape=(n + 1,)).copy()
+        nlist = np.ctypeslib.as_array(cg.nlist, shape=(m,)).copy() if m else np.zeros(0, np.int32)
+        ew = np.ctypeslib.as_array(cg.eweight, shape=(m,)).copy() if (cg.eweight and m) else None
+        if cg.eweight and m == 0:
+            ew = np.zeros(0, np.int32)
+    finally:
+        lib.ecl_graph_free(C.byref(cg))
+    return Graph(nindex, nlist, ew, symmetric)
+
+
+def read_graph(path: str) -> Graph:
+    """readECLgraph (library/ECLgraph.h:49-76), returning status instead of exiting."""
+    cg = CGraph()
+    _check(lib.ecl_graph_read(path.encode(), C.byref(cg)), f"ecl_graph_read({path})")
+    return _take(cg, False)
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 2, symmetrise: bool = True, weight_seed: int = 0, weight_max: int = 1 << 20) -> Graph:
+    cg = CGraph()
+    _check(lib.ecl_gen_rmat(scale, edge_factor, a, b, c, seed, int(symmetrise), weight_seed, weight_max, C.byref(cg)),
+           "ecl_gen_rmat")
+    return _take(cg, symmetrise)
+
+
+def gen_grid(rows: int, cols: int, delete_frac: float = 0.05, seed: int = 1, weight_seed: int = 0,
+             weight_max: int = 1 << 20) -> Graph:
+    cg = CGraph()
+    _check(lib.ecl_gen_grid(rows, cols, delete_frac, seed, weight_seed, weight_max, C.byref(cg)), "ecl_gen_grid")
+    return _take(cg, True)
+
+
+def gen_er(n: int, p: float, seed: int = 4, symmetrise: bool = False, weight_seed: int = 0,
+           weight_min: int = 1, weight_max: int = 1000) -> Graph:
+    cg = CGraph()
+    _check(lib.ecl_gen_er(n, p, seed, int(symmetrise), weight_seed, weight_min, weight_max, C.byref(cg)), "ecl_gen_er")
+    return _take(cg, symmetrise)
+
+
+@dataclass
+class DeviceGraph:
+    """CSR held in torch CUDA int32 tensors (torch is only the allocator here)."""
+
+    nindex: "object"
+    nlist: "object"
+    eweight: "object" = None
+    symmetric: bool = False
+    edges_: int = -1
+
+    @property
+    def nodes(self) -> int:
+        return int(self.nindex.shape[0] - 1)
+
+    @property
+    def edges(self) -> int:
+        return int(self.nlist.shape[0]) if self.edges_ < 0 else self.edges_
+
+    def view(self) -> GraphView:
+        v = GraphView()
+        v.nodes, v.edges = self.nodes, self.edges
+        v.nindex = self.nindex.data_ptr()
+        v.nlist = self.nlist.data_ptr()
+        v.eweight = self.eweight.data_ptr() if self.eweight is not None else None
+        v.location = DEVICE
+        v.flags = GRAPH_SYMMETRIC if self.symmetric else 0
+        return v
+
+
+# ---- solvers ---------------------------------------------------------------------
+
+
+def _opts(stream=None, workspace=None, validate=False, max_rounds=0) -> Opts:
+    o = Opts()
+    o.stream = stream
+    if workspace is not None:
+        o.workspace = workspace.data_ptr()
+        o.workspace_bytes = workspace.numel() * workspace.element_size()
+    o.validate = int(validate)
+    o.max_rounds = max_rounds
+    return o
+
+
+def workspace_bytes(code: int, nodes: int, edges: int) -> int:
+    return int(lib.ecl_workspace_bytes(code, nodes, edges))
+
+
+def _out(g, n, dtype, torch_dtype):
+    if isinstance(g, DeviceGraph):
+        import torch
+
+        return torch.empty(n, dtype=torch_dtype, device=g.nindex.device)
+    return np.empty(n, dtype=dtype)
+
+
+def _ptr(a) -> int:
+    return a.data_ptr() if hasattr(a, "data_ptr") else a.ctypes.data
+
+
+def _run(fn, name, g, out, *extra, opts: Optional[Opts] = None, **kw):
+    o = opts if opts is not None else _opts(**kw)
+    v = g.view()
+    _check(fn(C.byref(v), _ptr(out), *extra, C.byref(o)), name)
+    return o
+
+
+def cc(g, out=None, **kw):
+    """label[v] = smallest id in v's component (ECL-CC-atomic.cu:275 computeCC contract)."""
+    out = _out(g, g.nodes, np.int32, _torch_dtype("int32")) if out is None else out
+    _run(lib.ecl_cc, "ecl_cc", g, out, **kw)
+    return out
+
+
+def mis(g, out=None, **kw):
+    """status[v] in {0xfe, 0} (ECL-MIS-atomic.cu:147 computeMIS contract)."""
+    out = _out(g, g.nodes, np.uint8, _torch_dtype("uint8")) if out is None else out
+    _run(lib.ecl_mis, "ecl_mis", g, out, **kw)
+    return out
+
+
+def gc(g, out=None, **kw):
+    """color[v] >= 0, first-fit greedy in (degree, hash, id) priority (ECL-GC-atomic.cu:333-373)."""
+    out = _out(g, g.nodes, np.int32, _torch_dtype("int32")) if out is None else out
+    _run(lib.ecl_gc, "ecl_gc", g, out, **kw)
+    return out
+
+
+def mst(g, out=None, **kw):
+    """(in_mst[m] bytes, total weight) (ECL-MST_10-atomic.cu:285 gpuMST contract)."""
+    out = _out(g, max(g.edges, 1), np.uint8, _torch_dtype("uint8")) if out is None else out
+    total = C.c_uint64(0)
+    o = _opts(**kw) if "opts" not in kw else kw.pop("opts")
+    v = g.view()
+    _check(lib.ecl_mst(C.byref(v), _ptr(out), C.byref(total), C.byref(o)), "ecl_mst")
+    return out[: g.edges], int(total.value)
+
+
+def scc(g, out=None, **kw):
+    """label[v] = largest id in v's SCC (ECL-SCC_10-atomic.cu:318 readFirst(iomax[v]))."""
+    out = _out(g, g.nodes, np.int32, _torch_dtype("int32")) if out is None else out
+    _run(lib.ecl_scc, "ecl_scc", g, out, **kw)
+    return out
+
+
+def apsp(g, out=None, ld: Optional[int] = None, **kw):
+    """n x ld int32 distances (ECL-APSP-atomic.cu:460 FW_gpu_64 contract, unpadded)."""
+    n = g.nodes
+    ld = n if ld is None else ld
+    if out is None:
+        if isinstance(g, DeviceGraph):
+            import torch
+
+            out = torch.empty((n, ld), dtype=torch.int32, device=g.nindex.device)
+        else:
+            out = np.empty((n, ld), dtype=np.int32)
+    o = _opts(**kw) if "opts" not in kw else kw.pop("opts")
+    v = g.view()
+    _check(lib.ecl_apsp(C.byref(v), _ptr(out), ld, C.byref(o)), "ecl_apsp")
+    return out
+
+
+def _torch_dtype(name):
+    try:
+        import torch
+
+        return getattr(torch, name)
+    except ImportError:  # host-only use
+        return None
+
+
+def kernel_launches() -> int:
+    return int(lib.ecl_kernel_launches())

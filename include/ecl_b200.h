@@ -1,0 +1,216 @@
+/*
+ * ecl_b200.h -- C ABI of the B200-native race-free graph codes.
+ *
+ * One shared library (libeclb200.so) exports every entry point below with
+ * plain C types only: no CUDA, torch or C++ types cross this boundary, so the
+ * library can be bound from ctypes, cgo, JNI or plain C.
+ *
+ * The reference (ECL-Suite) ships six standalone executables and no library.
+ * Each entry point here replaces the internal host driver of one of them; the
+ * citation beside each declaration names the reference function (path:line
+ * within the ECL-Suite project) whose input/output contract it keeps.
+ *
+ * Conventions shared by every solver:
+ *  - The graph is the ECLgraph CSR (library/ECLgraph.h:41-47): int32 nodes,
+ *    int32 edges, nindex[nodes+1], nlist[edges], optional eweight[edges].
+ *  - `location` says where the CSR arrays AND the output arrays live.
+ *    ECL_HOST: the call copies the CSR to the device, solves, copies the
+ *    result back and returns with everything finished.  ECL_DEVICE: all
+ *    pointers are device pointers of the current CUDA device and nothing
+ *    crosses PCIe.
+ *  - Every call is stream-ordered on opts->stream (NULL = the legacy default
+ *    stream) and synchronises that stream before it returns, because the
+ *    device-side status word (non-convergence, bad input detected on the
+ *    device) is read back to form the return code.
+ *  - Errors are return codes; the library never calls exit() (the reference
+ *    does, library/ECLatomic.h:57-75).
+ *  - Scratch memory comes from opts->workspace when it is non-NULL and at
+ *    least ecl_workspace_bytes() large; otherwise the call allocates it
+ *    stream-ordered and frees it before returning.
+ */
+#ifndef ECL_B200_H
+#define ECL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECL_B200_ABI_VERSION 1
+
+typedef enum ecl_status {
+  ECL_OK = 0,
+  ECL_ERR_INVALID_ARG = 1,    /* NULL pointer, negative size, bad option */
+  ECL_ERR_BAD_GRAPH = 2,      /* CSR fails validation (nindex not monotone, id out of range, ...) */
+  ECL_ERR_OOM = 3,            /* device or host allocation failed, or workspace too small */
+  ECL_ERR_NO_CONVERGENCE = 4, /* a device fixpoint loop hit its round cap */
+  ECL_ERR_CUDA = 5,           /* a CUDA runtime call failed */
+  ECL_ERR_IO = 6,             /* file could not be opened, read or written */
+  ECL_ERR_UNSUPPORTED = 7,    /* input outside the supported range (e.g. APSP n too large) */
+  ECL_ERR_NO_DEVICE = 8       /* no CUDA device, or not an sm_100 device */
+} ecl_status;
+
+typedef enum ecl_location { ECL_HOST = 0, ECL_DEVICE = 1 } ecl_location;
+
+/* Graph flags (ecl_graph_view.flags). */
+#define ECL_GRAPH_SYMMETRIC 0x1 /* caller asserts that (u,v) in nlist implies (v,u) */
+
+typedef struct ecl_graph_view {
+  int32_t nodes;
+  int32_t edges;
+  const int32_t* nindex;  /* nodes + 1 entries, nindex[0] == 0, nindex[nodes] == edges */
+  const int32_t* nlist;   /* edges entries, each in [0, nodes) */
+  const int32_t* eweight; /* edges entries, or NULL when the graph has no weights */
+  int32_t location;       /* ecl_location of nindex/nlist/eweight and of the outputs */
+  int32_t flags;          /* ECL_GRAPH_* */
+} ecl_graph_view;
+
+typedef struct ecl_opts {
+  void* stream;           /* cudaStream_t; NULL = legacy default stream */
+  void* workspace;        /* device scratch, or NULL (the call allocates) */
+  size_t workspace_bytes; /* size of workspace */
+  int32_t validate;       /* 1: validate the CSR on the host before any launch */
+  int32_t max_rounds;     /* cap on device fixpoint rounds; 0 = built-in default */
+  float elapsed_ms;       /* out: device time of the compute phase (CUDA events) */
+  int32_t rounds;         /* out: fixpoint rounds / sweeps the solve took */
+} ecl_opts;
+
+/* Solver identifiers (ecl_workspace_bytes). */
+typedef enum ecl_code { ECL_CC = 0, ECL_MIS = 1, ECL_GC = 2, ECL_MST = 3, ECL_SCC = 4, ECL_APSP = 5 } ecl_code;
+
+/* MIS status bytes, as in src/racefree/egr-input/MIS/ECL-MIS-atomic.cu:67-68. */
+#define ECL_MIS_IN 0xfe
+#define ECL_MIS_OUT 0x00
+
+/* APSP "infinity", as in src/racefree/grid-input/ECL-APSP-atomic.cu:69. */
+#define ECL_APSP_INF (0x7fffffff / 2)
+
+/* ---- library ------------------------------------------------------------------ */
+
+int32_t ecl_abi_version(void);
+const char* ecl_status_string(ecl_status s);
+/* Text of the last CUDA/allocation failure seen by this thread ("" if none). */
+const char* ecl_last_error(void);
+/* Bytes of device scratch that `code` needs for a graph of this size. */
+size_t ecl_workspace_bytes(ecl_code code, int32_t nodes, int32_t edges);
+/* Number of this library's kernel launches since load (a process-wide counter). */
+uint64_t ecl_kernel_launches(void);
+
+/* ---- solvers ------------------------------------------------------------------ */
+
+/* Connected components.  label[v] = smallest vertex id in v's component, where
+ * the components are those of the undirected graph formed by the entries
+ * nlist[i] < v of each vertex v's list -- exactly the edges the reference
+ * hooks (src/racefree/egr-input/CC/ECL-CC-atomic.cu:114-153) -- so the labels
+ * equal the reference's nstat for every input, symmetric or not.
+ * Replaces computeCC (ECL-CC-atomic.cu:275). */
+ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* opts);
+
+/* Maximal independent set.  status[v] = ECL_MIS_IN (0xfe) or ECL_MIS_OUT (0).
+ * The set is the greedy MIS in descending (priority byte, vertex id) order,
+ * with the reference's hash priority (ECL-MIS-atomic.cu:109-136), i.e. the
+ * set the reference's findmins (ECL-MIS-atomic.cu:72-104) converges to.
+ * The graph must be symmetric and free of self-loops (the reference spins
+ * forever otherwise); opts->validate=1 checks this on the host.
+ * Replaces computeMIS (ECL-MIS-atomic.cu:147). */
+ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status, ecl_opts* opts);
+
+/* Graph colouring.  color[v] >= 0, adjacent vertices differ.  The colouring is
+ * first-fit greedy in the reference's priority order: degree, then hash, then
+ * id (ECL-GC-atomic.cu:102), which is what init/runLarge/runSmall
+ * (ECL-GC-atomic.cu:78-303) compute.  Graph must be symmetric, no self-loops.
+ * Replaces the GC driver inlined in main (ECL-GC-atomic.cu:333-373). */
+ecl_status ecl_gc(const ecl_graph_view* g, int32_t* color, ecl_opts* opts);
+
+/* Minimum spanning forest.  in_mst[j] = 1 for the CSR entries j (the v<n copy
+ * of each undirected edge, ECL-MST_10-atomic.cu:203) that form the unique
+ * minimum spanning forest under the (eweight, edge index) order, else 0.
+ * *total_weight (may be NULL) receives the forest weight.  Weights must be
+ * non-negative; only the v<n copy of each weight is read.
+ * Replaces gpuMST<filter> (ECL-MST_10-atomic.cu:285-382). */
+ecl_status ecl_mst(const ecl_graph_view* g, uint8_t* in_mst, uint64_t* total_weight, ecl_opts* opts);
+
+/* Strongly connected components of the directed graph.  label[v] = largest
+ * vertex id in v's SCC, the value the reference reads out as
+ * readFirst(iomax[v]) (ECL-SCC_10-atomic.cu:318).
+ * Replaces the SCC driver inlined in main (ECL-SCC_10-atomic.cu:240-311). */
+ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label, ecl_opts* opts);
+
+/* All-pairs shortest paths (Floyd-Warshall).  dist is nodes x ld int32,
+ * row-major, ld >= nodes; dist[i*ld+j] = shortest i->j distance, ECL_APSP_INF
+ * when unreachable.  The initial matrix follows init1/init2
+ * (ECL-APSP-atomic.cu:63-83): 0 on the diagonal, eweight[j] at
+ * (i, nlist[j]) with the LAST duplicate winning and a self-loop overwriting
+ * the 0.  Weights are used as given (the reference's main negates negative
+ * ones first, ECL-APSP-atomic.cu:586-590; the CLI drop-in does the same).
+ * Requires eweight.  Replaces FW_gpu_64 (ECL-APSP-atomic.cu:460-531). */
+ecl_status ecl_apsp(const ecl_graph_view* g, int32_t* dist, int64_t ld, ecl_opts* opts);
+
+/* ---- reference-shaped wrappers (host pointers, default stream) ---------------- */
+
+/* computeCC(nodes, edges, nidx, nlist, nstat), ECL-CC-atomic.cu:275 */
+ecl_status ecl_compute_cc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, int32_t* nstat);
+/* computeMIS(nodes, edges, nidx, nlist, nstat), ECL-MIS-atomic.cu:147 */
+ecl_status ecl_compute_mis(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, uint8_t* nstat);
+/* GC driver in main, ECL-GC-atomic.cu:333-373 */
+ecl_status ecl_compute_gc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, int32_t* color);
+/* gpuMST<filter>(g, threshold), ECL-MST_10-atomic.cu:285; the threshold is
+ * a performance knob in the reference and is chosen internally here. */
+ecl_status ecl_compute_mst(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, const int32_t* eweight, uint8_t* in_mst);
+/* SCC driver in main, ECL-SCC_10-atomic.cu:240-311 */
+ecl_status ecl_compute_scc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, int32_t* label);
+/* FW_gpu_64(g, AdjMat), ECL-APSP-atomic.cu:460: AdjMat is upper x upper with
+ * upper = ceil(nodes/64)*64, exactly the reference's padded output layout
+ * (padding rows/columns hold ECL_APSP_INF, as init1 leaves them). */
+ecl_status ecl_compute_apsp(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist, const int32_t* eweight, int32_t* adjmat);
+
+/* ---- ECLgraph files (library/ECLgraph.h:41-102) -------------------------------- */
+
+typedef struct ecl_graph {
+  int32_t nodes;
+  int32_t edges;
+  int32_t* nindex;
+  int32_t* nlist;
+  int32_t* eweight; /* NULL when the file has no weights */
+} ecl_graph;
+
+/* readECLgraph (ECLgraph.h:49-76): same byte layout and the same rejection of
+ * nodes < 1 or edges < 0, but returns ECL_ERR_IO / ECL_ERR_BAD_GRAPH instead of
+ * exiting.  Arrays are malloc'ed; release with ecl_graph_free. */
+ecl_status ecl_graph_read(const char* path, ecl_graph* out);
+/* writeECLgraph (ECLgraph.h:78-92): byte-identical output. */
+ecl_status ecl_graph_write(const char* path, const ecl_graph* g);
+/* freeECLgraph (ECLgraph.h:94-102). */
+void ecl_graph_free(ecl_graph* g);
+
+/* Host-side CSR checks.  require_symmetric / forbid_self_loops add those
+ * checks (O(edges log deg)); returns ECL_OK or ECL_ERR_BAD_GRAPH. */
+ecl_status ecl_graph_validate(const ecl_graph_view* g, int32_t require_symmetric, int32_t forbid_self_loops);
+
+/* ---- seeded synthetic generators (host, deterministic for any thread count) ---- */
+
+/* R-MAT: 2^scale vertices, edge_factor * 2^scale sampled edges with quadrant
+ * probabilities (a, b, c, 1-a-b-c).  symmetrise=1 adds both directions.
+ * Self-loops and duplicates are always removed; lists are sorted.
+ * weight_seed != 0 attaches weights uniform in [1, weight_max), symmetric per
+ * unordered pair.  The graph is malloc'ed; release with ecl_graph_free. */
+ecl_status ecl_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                        int32_t symmetrise, uint64_t weight_seed, int32_t weight_max, ecl_graph* out);
+/* 2D rows x cols 4-neighbour grid, undirected; each undirected edge is deleted
+ * independently with probability delete_frac (seed). */
+ecl_status ecl_gen_grid(int32_t rows, int32_t cols, double delete_frac, uint64_t seed, uint64_t weight_seed,
+                        int32_t weight_max, ecl_graph* out);
+/* Erdos-Renyi G(n, p).  symmetrise=0: each ordered pair (i != j) independently
+ * (a directed graph); symmetrise=1: each unordered pair, stored both ways.
+ * Weights uniform in [weight_min, weight_max] inclusive when weight_seed != 0
+ * (independent per directed entry when symmetrise=0, per pair otherwise). */
+ecl_status ecl_gen_er(int32_t n, double p, uint64_t seed, int32_t symmetrise, uint64_t weight_seed,
+                      int32_t weight_min, int32_t weight_max, ecl_graph* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ECL_B200_H */

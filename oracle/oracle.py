@@ -1,0 +1,116 @@
+"""ctypes wrapper of the CPU oracle (oracle.c) -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+legs import this module.  It is the checker, never the thing measured or
+shipped; the product library has no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"oracle not built at {LIB_PATH}; run `make -C oracle`")
+_lib = C.CDLL(LIB_PATH)
+
+_P = C.c_void_p
+for name, res, args in [
+    ("orc_cc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_verify_cc", C.c_int, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_mis_priority", None, [C.c_int, C.c_int, _P, _P]),
+    ("orc_mis", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_verify_mis", C.c_int, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_gc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_verify_gc", C.c_int, [C.c_int, C.c_int, _P, _P, _P, C.POINTER(C.c_int)]),
+    ("orc_mst", C.c_uint64, [C.c_int, C.c_int, _P, _P, _P, _P]),
+    ("orc_scc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("orc_apsp", None, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_long]),
+]:
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = args
+
+
+def _arrs(g):
+    nindex = np.ascontiguousarray(g.nindex, dtype=np.int32)
+    nlist = np.ascontiguousarray(g.nlist, dtype=np.int32)
+    if nlist.size == 0:
+        nlist = np.zeros(1, np.int32)
+    return int(nindex.shape[0] - 1), int(g.nlist.shape[0]), nindex, nlist
+
+
+def cc(g) -> np.ndarray:
+    n, m, ni, nl = _arrs(g)
+    out = np.empty(n, np.int32)
+    _lib.orc_cc(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def verify_cc(g, label) -> int:
+    n, m, ni, nl = _arrs(g)
+    lab = np.ascontiguousarray(label, dtype=np.int32)
+    return _lib.orc_verify_cc(n, m, ni.ctypes.data, nl.ctypes.data, lab.ctypes.data)
+
+
+def mis_priority(g) -> np.ndarray:
+    n, m, ni, _ = _arrs(g)
+    out = np.empty(n, np.uint8)
+    _lib.orc_mis_priority(n, m, ni.ctypes.data, out.ctypes.data)
+    return out
+
+
+def mis(g) -> np.ndarray:
+    n, m, ni, nl = _arrs(g)
+    out = np.empty(n, np.uint8)
+    _lib.orc_mis(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def verify_mis(g, status) -> int:
+    n, m, ni, nl = _arrs(g)
+    st = np.ascontiguousarray(status, dtype=np.uint8)
+    return _lib.orc_verify_mis(n, m, ni.ctypes.data, nl.ctypes.data, st.ctypes.data)
+
+
+def gc(g) -> np.ndarray:
+    n, m, ni, nl = _arrs(g)
+    out = np.empty(n, np.int32)
+    _lib.orc_gc(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def verify_gc(g, color):
+    """Returns (rc, number of colours)."""
+    n, m, ni, nl = _arrs(g)
+    col = np.ascontiguousarray(color, dtype=np.int32)
+    k = C.c_int(0)
+    rc = _lib.orc_verify_gc(n, m, ni.ctypes.data, nl.ctypes.data, col.ctypes.data, C.byref(k))
+    return rc, k.value
+
+
+def mst(g):
+    """Returns (in_mst bytes, total weight)."""
+    n, m, ni, nl = _arrs(g)
+    w = np.ascontiguousarray(g.eweight, dtype=np.int32) if m else np.zeros(1, np.int32)
+    out = np.zeros(max(m, 1), np.uint8)
+    total = _lib.orc_mst(n, m, ni.ctypes.data, nl.ctypes.data, w.ctypes.data, out.ctypes.data)
+    return out[:m], int(total)
+
+
+def scc(g) -> np.ndarray:
+    n, m, ni, nl = _arrs(g)
+    out = np.empty(n, np.int32)
+    _lib.orc_scc(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def apsp(g) -> np.ndarray:
+    n, m, ni, nl = _arrs(g)
+    w = np.ascontiguousarray(g.eweight, dtype=np.int32) if m else np.zeros(1, np.int32)
+    out = np.empty((n, n), np.int32)
+    _lib.orc_apsp(n, m, ni.ctypes.data, nl.ctypes.data, w.ctypes.data, out.ctypes.data, n)
+    return out

@@ -1,0 +1,73 @@
+"""The CPU oracle on hand-checked graphs and against the reference's own
+self-checks (CPU only).  Fixture-based pins live in test_golden.py."""
+import numpy as np
+
+from conftest import from_edges, undirected
+
+
+def test_cc_hand(orc):
+    g = undirected(7, [(0, 3), (3, 5), (1, 2), (6, 2)])
+    assert list(orc.cc(g)) == [0, 1, 1, 0, 4, 0, 1]
+    assert orc.verify_cc(g, orc.cc(g)) == 0
+    assert orc.verify_cc(g, np.array([0, 1, 1, 0, 4, 0, 2], np.int32)) != 0
+
+
+def test_cc_asymmetric_uses_smaller_entries_only(orc):
+    # 2 -> 0 is a "smaller" entry (hooked); 1 -> 3 is not (ignored), as in
+    # ECL-CC-atomic.cu:132.
+    g = from_edges(4, [(2, 0), (1, 3)])
+    assert list(orc.cc(g)) == [0, 1, 0, 3]
+
+
+def test_mis_priority_formula(orc):
+    g = undirected(4, [(0, 1), (1, 2), (2, 3)])
+    p = orc.mis_priority(g)
+    assert all(int(x) & 1 for x in p)
+    iso = undirected(3, [(0, 1)])
+    assert orc.mis_priority(iso)[2] == 0xFE
+
+
+def test_mis_greedy_and_verify(orc, ecl):
+    g = ecl.gen_rmat(10, 8, seed=7)
+    st = orc.mis(g)
+    assert orc.verify_mis(g, st) == 0
+    p = orc.mis_priority(g)
+    # the highest (byte, id) vertex with degree > 0 is always in the set
+    deg = np.diff(g.nindex)
+    cand = [v for v in range(g.nodes) if deg[v] > 0]
+    top = max(cand, key=lambda v: (int(p[v]), v))
+    assert st[top] == 0xFE
+
+
+def test_gc_greedy_and_verify(orc, ecl):
+    g = ecl.gen_rmat(10, 8, seed=8)
+    col = orc.gc(g)
+    rc, k = orc.verify_gc(g, col)
+    assert rc == 0 and k >= 2
+    assert orc.verify_gc(g, np.zeros(g.nodes, np.int32))[0] != 0
+
+
+def test_mst_hand(orc):
+    # square with a diagonal; unique by (w, j)
+    g = undirected(4, [(0, 1), (1, 2), (2, 3), (3, 0), (0, 2)], weights=[1, 1, 5, 1, 1])
+    inm, tot = orc.mst(g)
+    assert tot == 3 and int(inm.sum()) == 3
+    # only v<n copies are flagged
+    src = np.repeat(np.arange(4), np.diff(g.nindex))
+    assert all(g.nlist[j] > src[j] for j in np.nonzero(inm)[0])
+
+
+def test_scc_hand(orc):
+    g = from_edges(6, [(0, 1), (1, 2), (2, 0), (2, 3), (3, 4), (4, 3), (5, 5)])
+    assert list(orc.scc(g)) == [2, 2, 2, 4, 4, 5]
+
+
+def test_apsp_hand(orc):
+    INF = 0x7FFFFFFF // 2
+    g = from_edges(3, [(0, 1), (1, 2), (0, 2), (0, 2)], weights=[2, 3, 9, 7])
+    d = orc.apsp(g)
+    assert d[0, 2] == 5 and d[0, 1] == 2 and d[1, 2] == 3
+    assert d[2, 0] == INF and d[1, 1] == 0
+    # a self-loop overwrites the 0 diagonal (init2, ECL-APSP-atomic.cu:79)
+    s = from_edges(2, [(0, 0), (0, 1)], weights=[4, 1])
+    assert orc.apsp(s)[0, 0] == 4
