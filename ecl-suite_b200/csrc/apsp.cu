@@ -1,0 +1,340 @@
+// All-pairs shortest paths, blocked Floyd-Warshall (ECL-APSP contract).
+//
+// Result contract (src/racefree/grid-input/ECL-APSP-atomic.cu): the matrix
+// starts as init1/init2 build it (:63-83) -- 0 on the diagonal of real
+// vertices, INF = INT_MAX/2 elsewhere (padding included), then each list entry
+// j of row i writes eweight[j] at (i, nlist[j]) in CSR order (last duplicate
+// wins, a self-loop replaces the 0) -- and ends as the Floyd-Warshall closure
+// FW_cpu computes (:533-570).  With non-negative weights every entry of that
+// closure is min(INF, shortest-path length), which any correct blocked
+// schedule reproduces exactly: int32 add+min, no rounding, and
+// INF/2 + INF/2 < INT_MAX so no sum overflows.
+//
+// B200 design.  Min-plus is not a ring product, so the tensor cores cannot do
+// it; the kernel is INT32-pipe bound.  Per 128-wide k-block kb:
+//  * apsp_panels: CTA 0 closes the 128x128 diagonal tile in registers (one
+//    barrier per k, row/column k double-buffered in shared memory) and stores
+//    it to a side buffer; every other CTA recomputes the same closure
+//    (cheaper than a launch + global round trip) and then updates one row
+//    panel tile (D (x) tile) or one column panel tile (tile (x) D);
+//  * apsp_update: every remaining tile C = min(C, A[i][kb] (x) A[kb][j]),
+//    K split in two 64-wide chunks so two CTAs fit per SM; one extra CTA
+//    installs the closed diagonal tile (no CTA reads a tile another CTA of
+//    the same launch writes).
+// The tile product keeps an 8x8 register tile per thread (256 threads),
+// reads A as 128-bit rows along k and B as 128-bit rows along j from shared
+// memory (A rows padded by 4 words: conflict-free), and issues one DPX
+// __viaddmin_s32 = min(a + b, c) per update.
+#include "runtime.cuh"
+
+namespace ecl {
+namespace {
+
+using namespace dev;
+
+constexpr int kT = 128;        // tile edge
+constexpr int kThreads = 256;  // 16 x 16 threads, 8 x 8 cells each
+constexpr int kKC = 64;        // k-chunk of apsp_update
+constexpr int kPadA = 4;
+constexpr int kInf = 0x7fffffff / 2;
+
+// Row (r in 0..7) and column (c in 0..7) of a thread's cell within a tile.
+__device__ __forceinline__ int cell_row(int ty, int r) { return (r < 4) ? ty * 4 + r : 64 + ty * 4 + (r - 4); }
+__device__ __forceinline__ int cell_col(int tx, int c) { return (c < 4) ? tx * 4 + c : 64 + tx * 4 + (c - 4); }
+
+// acc[r][c] = min(acc[r][c], min_k As[row_r][k] + Bs[k][col_c]), k in [0, K).
+template <int K>
+__device__ __forceinline__ void minplus_tile(const int* __restrict__ As, int lda, const int* __restrict__ Bs, int ldb,
+                                             int (&acc)[8][8], int ty, int tx) {
+#pragma unroll 1
+  for (int k = 0; k < K; k += 4) {
+    int a[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      const int4 t = *reinterpret_cast<const int4*>(&As[cell_row(ty, r) * lda + k]);
+      a[r][0] = t.x;
+      a[r][1] = t.y;
+      a[r][2] = t.z;
+      a[r][3] = t.w;
+    }
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      const int4 b0 = *reinterpret_cast<const int4*>(&Bs[(k + kk) * ldb + tx * 4]);
+      const int4 b1 = *reinterpret_cast<const int4*>(&Bs[(k + kk) * ldb + 64 + tx * 4]);
+      const int b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int r = 0; r < 8; r++) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) acc[r][c] = __viaddmin_s32(a[r][kk], b[c], acc[r][c]);
+      }
+    }
+  }
+}
+
+// Loads a 128 x 128 tile at (row0, col0) of the global matrix into registers.
+__device__ __forceinline__ void load_acc(const int* A, long ld, int row0, int col0, int (&acc)[8][8], int ty, int tx) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    const int* p = A + (long)(row0 + cell_row(ty, r)) * ld + col0;
+    const int4 x = *reinterpret_cast<const int4*>(p + tx * 4);
+    const int4 y = *reinterpret_cast<const int4*>(p + 64 + tx * 4);
+    acc[r][0] = x.x; acc[r][1] = x.y; acc[r][2] = x.z; acc[r][3] = x.w;
+    acc[r][4] = y.x; acc[r][5] = y.y; acc[r][6] = y.z; acc[r][7] = y.w;
+  }
+}
+
+__device__ __forceinline__ void store_acc(int* A, long ld, int row0, int col0, const int (&acc)[8][8], int ty, int tx) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    int* p = A + (long)(row0 + cell_row(ty, r)) * ld + col0;
+    *reinterpret_cast<int4*>(p + tx * 4) = make_int4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+    *reinterpret_cast<int4*>(p + 64 + tx * 4) = make_int4(acc[r][4], acc[r][5], acc[r][6], acc[r][7]);
+  }
+}
+
+__device__ __forceinline__ void acc_to_smem(int* S, int lds, const int (&acc)[8][8], int ty, int tx) {
+#pragma unroll
+  for (int r = 0; r < 8; r++) {
+    int* p = S + cell_row(ty, r) * lds;
+    *reinterpret_cast<int4*>(p + tx * 4) = make_int4(acc[r][0], acc[r][1], acc[r][2], acc[r][3]);
+    *reinterpret_cast<int4*>(p + 64 + tx * 4) = make_int4(acc[r][4], acc[r][5], acc[r][6], acc[r][7]);
+  }
+}
+
+// Copies a rows x cols (cols % 4 == 0) block of the global matrix into shared
+// memory with leading dimension lds.
+__device__ __forceinline__ void gmem_to_smem(const int* A, long ld, int row0, int col0, int rows, int cols, int* S,
+                                             int lds) {
+  const int vec_per_row = cols / 4;
+  for (int q = threadIdx.x; q < rows * vec_per_row; q += kThreads) {
+    const int r = q / vec_per_row, c4 = q % vec_per_row;
+    *reinterpret_cast<int4*>(&S[r * lds + c4 * 4]) =
+        *reinterpret_cast<const int4*>(&A[(long)(row0 + r) * ld + col0 + c4 * 4]);
+  }
+}
+
+// Floyd-Warshall closure of the diagonal tile held in acc; leaves the closed
+// tile in acc.  rowbuf/colbuf: 2 x 128 ints each (double-buffered row/col k).
+__device__ __forceinline__ void close_diag(int (&acc)[8][8], int* rowbuf, int* colbuf, int ty, int tx) {
+  // publish row 0 and column 0
+  auto publish = [&](int k, int buf) {
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+      if (cell_row(ty, r) == k) {
+#pragma unroll
+        for (int c = 0; c < 8; c++) rowbuf[buf * kT + cell_col(tx, c)] = acc[r][c];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      if (cell_col(tx, c) == k) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) colbuf[buf * kT + cell_row(ty, r)] = acc[r][c];
+      }
+    }
+  };
+  publish(0, 0);
+  __syncthreads();
+#pragma unroll 1
+  for (int k = 0; k < kT; k++) {
+    const int buf = k & 1;
+    int col[8], row[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) col[r] = colbuf[buf * kT + cell_row(ty, r)];
+#pragma unroll
+    for (int c = 0; c < 8; c++) row[c] = rowbuf[buf * kT + cell_col(tx, c)];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+#pragma unroll
+      for (int c = 0; c < 8; c++) acc[r][c] = __viaddmin_s32(col[r], row[c], acc[r][c]);
+    }
+    if (k + 1 < kT) publish(k + 1, buf ^ 1);
+    __syncthreads();
+  }
+}
+
+// Dynamic shared memory of apsp_panels: D (128 x 132) + operand (128 x 132)
+// + row/col buffers.
+constexpr int kLdP = kT + kPadA;
+constexpr size_t kPanelSmem = sizeof(int) * (size_t)(2 * kT * kLdP + 4 * kT);
+
+// The closed diagonal tile goes to Dout (a separate 128 x 128 buffer) when
+// nb > 1, because the other CTAs of this launch still read the original tile;
+// apsp_update's last CTA copies it into place.
+__global__ void __launch_bounds__(kThreads, 1) apsp_panels(int* __restrict__ A, long ld, int nb, int kb,
+                                                           int* __restrict__ Dout) {
+  extern __shared__ __align__(16) int smem[];
+  int* D = smem;
+  int* X = smem + kT * kLdP;
+  int* rowbuf = X + kT * kLdP;
+  int* colbuf = rowbuf + 2 * kT;
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  const int k0 = kb * kT;
+  int acc[8][8];
+  load_acc(A, ld, k0, k0, acc, ty, tx);
+  close_diag(acc, rowbuf, colbuf, ty, tx);
+  if (blockIdx.x == 0) {
+    if (nb == 1) store_acc(A, ld, k0, k0, acc, ty, tx);
+    else store_acc(Dout, kT, 0, 0, acc, ty, tx);
+    return;
+  }
+  acc_to_smem(D, kLdP, acc, ty, tx);
+  const int p = blockIdx.x - 1;
+  if (p < nb - 1) {
+    // row panel tile (kb, j): acc = min(acc, D (x) tile)
+    const int j = (p >= kb) ? p + 1 : p;
+    const int c0 = j * kT;
+    gmem_to_smem(A, ld, k0, c0, kT, kT, X, kLdP);
+    __syncthreads();
+    load_acc(A, ld, k0, c0, acc, ty, tx);
+    minplus_tile<kT>(D, kLdP, X, kLdP, acc, ty, tx);
+    store_acc(A, ld, k0, c0, acc, ty, tx);
+  } else {
+    // column panel tile (i, kb): acc = min(acc, tile (x) D)
+    const int q = p - (nb - 1);
+    const int i = (q >= kb) ? q + 1 : q;
+    const int r0 = i * kT;
+    gmem_to_smem(A, ld, r0, k0, kT, kT, X, kLdP);
+    __syncthreads();
+    load_acc(A, ld, r0, k0, acc, ty, tx);
+    minplus_tile<kT>(X, kLdP, D, kLdP, acc, ty, tx);
+    store_acc(A, ld, r0, k0, acc, ty, tx);
+  }
+}
+
+constexpr int kLdA = kKC + kPadA;
+constexpr size_t kUpdateSmem = sizeof(int) * (size_t)(kT * kLdA + kKC * kT);
+
+__global__ void __launch_bounds__(kThreads, 2) apsp_update(int* __restrict__ A, long ld, int nb, int kb,
+                                                           const int* __restrict__ Dclosed) {
+  extern __shared__ __align__(16) int smem[];
+  int* As = smem;              // [128][kLdA]  column panel slice A[i][kb]
+  int* Bs = smem + kT * kLdA;  // [kKC][128]   row panel slice A[kb][j]
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+  const int nm1 = nb - 1;
+  if (blockIdx.x == nm1 * nm1) {  // last CTA: install the closed diagonal tile
+    int acc[8][8];
+    load_acc(Dclosed, kT, 0, 0, acc, ty, tx);
+    store_acc(A, ld, kb * kT, kb * kT, acc, ty, tx);
+    return;
+  }
+  int bi = blockIdx.x / nm1, bj = blockIdx.x % nm1;
+  if (bi >= kb) bi++;
+  if (bj >= kb) bj++;
+  const int r0 = bi * kT, c0 = bj * kT, k0 = kb * kT;
+  int acc[8][8];
+  load_acc(A, ld, r0, c0, acc, ty, tx);
+#pragma unroll 1
+  for (int kc = 0; kc < kT; kc += kKC) {
+    gmem_to_smem(A, ld, r0, k0 + kc, kT, kKC, As, kLdA);
+    gmem_to_smem(A, ld, k0 + kc, c0, kKC, kT, Bs, kT);
+    __syncthreads();
+    minplus_tile<kKC>(As, kLdA, Bs, kT, acc, ty, tx);
+    __syncthreads();
+  }
+  store_acc(A, ld, r0, c0, acc, ty, tx);
+}
+
+__global__ void apsp_fill(int* __restrict__ A, long ld, int N, int n) {
+  const long total4 = (long)N * N / 4;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total4; q += (long)gridDim.x * blockDim.x) {
+    const long idx = q * 4;
+    const int i = (int)(idx / N), j = (int)(idx % N);
+    int4 v = make_int4(kInf, kInf, kInf, kInf);
+    if (i < n && i >= j && i < j + 4) (&v.x)[i - j] = 0;
+    *reinterpret_cast<int4*>(&A[(long)i * ld + j]) = v;
+  }
+}
+
+// One thread per row writes the row's entries in CSR order, so the last
+// duplicate wins exactly as in init2 (ECL-APSP-atomic.cu:74-83).
+__global__ void apsp_edges(int* __restrict__ A, long ld, int n, int m, const int* __restrict__ nindex,
+                           const int* __restrict__ nlist, const int* __restrict__ eweight, Status* __restrict__ status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int beg = __ldg(&nindex[i]), end = __ldg(&nindex[i + 1]);
+    if (beg < 0 || end < beg || end > m) {
+      raise(status, ECL_ERR_BAD_GRAPH, i);
+      continue;
+    }
+    for (int j = beg; j < end; j++) {
+      const int u = __ldg(&nlist[j]);
+      const int w = __ldg(&eweight[j]);
+      if ((unsigned)u >= (unsigned)n || w < 0) {
+        raise(status, ECL_ERR_BAD_GRAPH, j);
+        continue;
+      }
+      A[(long)i * ld + u] = w;
+    }
+  }
+}
+
+}  // namespace
+
+int apsp_padded(int n) { return (n + kT - 1) / kT * kT; }
+
+size_t apsp_workspace_bytes(int n, int m) {
+  (void)m;
+  const size_t N = (size_t)apsp_padded(n);
+  return (N * N + (size_t)kT * kT) * sizeof(int);
+}
+
+}  // namespace ecl
+
+extern "C" ecl_status ecl_apsp(const ecl_graph_view* g, int32_t* dist, int64_t ld, ecl_opts* opts) {
+  using namespace ecl;
+  ecl_opts local{};
+  if (!opts) opts = &local;
+  if (!dist || !g || ld < g->nodes) return ECL_ERR_INVALID_ARG;
+  if (g->nodes > 46340 * 2) return ECL_ERR_UNSUPPORTED;  // N^2 int32 must stay addressable and < HBM
+  const int N = apsp_padded(g->nodes);
+  // Work in place when the caller's device matrix already has the padded shape.
+  const bool inplace = g->location == ECL_DEVICE && N == g->nodes && ld == N;
+  Solve s(g, opts);
+  GraphNeeds needs;
+  needs.weights = true;
+  const size_t dbytes = sizeof(int) * (size_t)kT * kT;
+  ecl_status st = s.begin(needs, inplace ? dbytes : apsp_workspace_bytes(g->nodes, g->edges));
+  if (st != ECL_OK) return s.finish(st);
+  int* Dbuf = reinterpret_cast<int*>(s.ws);
+  int* W = inplace ? dist : reinterpret_cast<int*>(s.ws + dbytes);
+  const int nb = N / kT;
+  static bool attr_set[64] = {false};
+  if (!attr_set[s.dev.device & 63]) {
+    if (cudaFuncSetAttribute(apsp_panels, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmem) != cudaSuccess ||
+        cudaFuncSetAttribute(apsp_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem) != cudaSuccess)
+      return s.finish(ECL_ERR_CUDA);
+    attr_set[s.dev.device & 63] = true;
+  }
+  const int grid = s.dev.sms * 4;
+
+  s.start_timer();
+  ECL_LAUNCH(apsp_fill, grid, 256, 0, s.stream, W, (long)N, N, s.n);
+  if (s.m > 0) ECL_LAUNCH(apsp_edges, (s.n + 255) / 256, 256, 0, s.stream, W, (long)N, s.n, s.m, s.nindex, s.nlist, s.eweight, s.status);
+  for (int kb = 0; kb < nb; kb++) {
+    ECL_LAUNCH(apsp_panels, 1 + 2 * (nb - 1), kThreads, kPanelSmem, s.stream, W, (long)N, nb, kb, Dbuf);
+    if (nb > 1)
+      ECL_LAUNCH(apsp_update, (nb - 1) * (nb - 1) + 1, kThreads, kUpdateSmem, s.stream, W, (long)N, nb, kb, Dbuf);
+  }
+  s.stop_timer();
+  if (!inplace) {
+    const cudaMemcpyKind kind = g->location == ECL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (cudaMemcpy2DAsync(dist, (size_t)ld * sizeof(int), W, (size_t)N * sizeof(int), (size_t)s.n * sizeof(int),
+                          (size_t)s.n, kind, s.stream) != cudaSuccess)
+      return s.finish(ECL_ERR_CUDA);
+  }
+  return s.finish();
+}
+
+extern "C" ecl_status ecl_compute_apsp(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,
+                                       const int32_t* eweight, int32_t* adjmat) {
+  if (nodes < 1 || !adjmat) return ECL_ERR_INVALID_ARG;
+  const int64_t upper = ((int64_t)nodes + 63) / 64 * 64;  // the reference's padded layout
+  ecl_graph_view g{nodes, edges, nidx, nlist, eweight, ECL_HOST, 0};
+  ecl_opts o{};
+  const ecl_status st = ecl_apsp(&g, adjmat, upper, &o);
+  if (st != ECL_OK) return st;
+  for (int64_t i = 0; i < upper; i++) {
+    for (int64_t j = (i < nodes ? nodes : 0); j < upper; j++) adjmat[i * upper + j] = ECL_APSP_INF;
+  }
+  return ECL_OK;
+}

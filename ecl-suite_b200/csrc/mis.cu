@@ -1,0 +1,252 @@
+// Maximal independent set (ECL-MIS contract).
+//
+// Result contract (src/racefree/egr-input/MIS/ECL-MIS-atomic.cu): every
+// vertex has a fixed priority byte (:118-136); findmins (:72-104) lets an
+// undecided vertex join once every undecided neighbour has a lower
+// (byte, id) and none is in.  With fixed priorities the set this converges to
+// is the sequential greedy MIS in descending (byte, id) order, independent of
+// the schedule, so the set below is bit-identical.
+//
+// B200 design:
+//  * status bytes packed four per 32-bit word in the workspace (4.2 MB at
+//    R-MAT-22, resident in the 126 MB L2); every shared access is a
+//    device-scope relaxed atomic on the word;
+//  * mis_init computes the priority bytes with the reference's fp32 formula
+//    using explicit round-to-nearest intrinsics (no contraction);
+//  * mis_run is ONE persistent launch: each warp sweeps its vertex groups
+//    until all are decided.  Lists of <= 32 entries are scanned by their own
+//    lane with an early exit at the first blocker; longer lists are scanned
+//    32 entries per step by the whole warp (two ballots per step); a joining
+//    vertex claims itself with one CAS, then clears its neighbours' bytes
+//    (fetch_and), so blocked neighbours see OUT without rescanning;
+//  * a sweep cap turns a non-converging input (self-loop, asymmetric list --
+//    the reference spins forever there) into ECL_ERR_NO_CONVERGENCE.
+#include "runtime.cuh"
+
+namespace ecl {
+namespace {
+
+using namespace dev;
+
+constexpr int kTPB = 256;
+constexpr int kLaneMax = 32;
+constexpr unsigned kIn = 0xfe;
+
+__device__ __forceinline__ unsigned byte_of(unsigned word, int v) { return (word >> ((v & 3) * 8)) & 0xffu; }
+
+__device__ __forceinline__ unsigned mis_priority(int v, int degree, float avg, float scaledavg) {
+  if (degree <= 0) return kIn;
+  // x = degree - hash(v) * 2^-32 ; res = rint(scaledavg / (avg + x))
+  const float h = __fmul_rn(__uint2float_rn(ecl_hash((unsigned)v)), 0.00000000023283064365386962890625f);
+  const float x = __fsub_rn(__int2float_rn(degree), h);
+  const int res = __float2int_rn(__fdiv_rn(scaledavg, __fadd_rn(avg, x)));
+  return (unsigned)((res + res) | 1) & 0xffu;
+}
+
+__global__ void __launch_bounds__(kTPB) mis_init(int n, int m, const int* __restrict__ nindex,
+                                                 unsigned* __restrict__ st4, int nwords, Status* __restrict__ status) {
+  const float avg = __fdiv_rn(__int2float_rn(m), __int2float_rn(n));
+  const float scaledavg = __fmul_rn(126.0f, avg);
+  for (int w = blockIdx.x * kTPB + threadIdx.x; w < nwords; w += gridDim.x * kTPB) {
+    unsigned word = 0;
+    for (int k = 0; k < 4; k++) {
+      const int v = 4 * w + k;
+      unsigned b = 0;  // padding vertices are OUT
+      if (v < n) {
+        const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
+        if (beg < 0 || end < beg || end > m) raise(status, ECL_ERR_BAD_GRAPH, v);
+        b = mis_priority(v, end - beg, avg, scaledavg);
+      }
+      word |= b << (8 * k);
+    }
+    st4[w] = word;
+  }
+}
+
+// Outcome of scanning v's list.
+enum : int { kWait = 0, kJoin = 1, kOut = 2 };
+
+// Per-neighbour verdict: IN neighbour -> v is out; undecided neighbour with
+// a higher (byte, id) -> v must wait; else no constraint.
+__device__ __forceinline__ int mis_verdict(unsigned sb, unsigned b, int u, int v) {
+  if (sb == kIn) return kOut;
+  if ((sb & 1u) && (sb > b || (sb == b && u > v))) return kWait;
+  return kJoin;
+}
+
+// Claims v as IN if its byte is still the undecided value b.
+__device__ __forceinline__ bool mis_claim(unsigned* st4, int v, unsigned b) {
+  unsigned* word = &st4[v >> 2];
+  const int sh = (v & 3) * 8;
+  unsigned cur = ld(word);
+  while (byte_of(cur, v) == b) {
+    const unsigned want = (cur & ~(0xffu << sh)) | (kIn << sh);
+    const unsigned seen = cas(word, cur, want);
+    if (seen == cur) return true;
+    cur = seen;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mis_set_out(unsigned* st4, int u) { fetch_and(&st4[u >> 2], ~(0xffu << ((u & 3) * 8))); }
+
+__global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restrict__ nindex,
+                                                const int* __restrict__ nlist, unsigned* __restrict__ st4,
+                                                Status* __restrict__ status, int max_sweeps) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  int sweep = 0;
+  for (;; sweep++) {
+    bool missing = false;
+    for (int base = warp * 32; base < n; base += nwarps * 32) {
+      const int v = base + lane;
+      unsigned b = 0;
+      if (v < n) b = byte_of(ld(&st4[v >> 2]), v);
+      const bool und = (b & 1u) != 0;
+      if (!__any_sync(kFull, und)) continue;
+      int beg = 0, end = 0;
+      if (und) {
+        beg = __ldg(&nindex[v]);
+        end = __ldg(&nindex[v + 1]);
+        if (beg < 0 || end < beg || end > m) beg = end = 0;  // reported by mis_init
+      }
+      const bool big = und && (end - beg) > kLaneMax;
+      int verdict = kWait;
+      if (und && !big) {
+        verdict = kJoin;
+        for (int i = beg; i < end; i++) {
+          const int u = __ldg(&nlist[i]);
+          if ((unsigned)u >= (unsigned)n) {
+            raise(status, ECL_ERR_BAD_GRAPH, u);
+            continue;
+          }
+          const int r = mis_verdict(byte_of(ld(&st4[u >> 2]), u), b, u, v);
+          if (r != kJoin) {
+            verdict = r;
+            break;
+          }
+        }
+        if (verdict == kJoin) {
+          if (mis_claim(st4, v, b)) {
+            for (int i = beg; i < end; i++) {
+              const int u = __ldg(&nlist[i]);
+              if ((unsigned)u < (unsigned)n) mis_set_out(st4, u);
+            }
+          }
+        } else if (verdict == kOut) {
+          mis_set_out(st4, v);
+        }
+      }
+      // Long lists: the whole warp scans one list, 32 entries per step.
+      unsigned todo = __ballot_sync(kFull, big);
+      while (todo) {
+        const int who = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int wv = __shfl_sync(kFull, v, who);
+        const int wbeg = __shfl_sync(kFull, beg, who);
+        const int wend = __shfl_sync(kFull, end, who);
+        const unsigned wb = __shfl_sync(kFull, b, who);
+        int wverdict = kJoin;
+        for (int i0 = wbeg; i0 < wend; i0 += 32) {
+          const int i = i0 + lane;
+          int r = kJoin;
+          if (i < wend) {
+            const int u = __ldg(&nlist[i]);
+            if ((unsigned)u < (unsigned)n) {
+              r = mis_verdict(byte_of(ld(&st4[u >> 2]), u), wb, u, wv);
+            } else {
+              raise(status, ECL_ERR_BAD_GRAPH, u);
+            }
+          }
+          if (__any_sync(kFull, r == kOut)) {
+            wverdict = kOut;
+            break;
+          }
+          if (__any_sync(kFull, r == kWait)) {
+            wverdict = kWait;
+            break;
+          }
+        }
+        if (wverdict == kJoin) {
+          bool claimed = false;
+          if (lane == 0) claimed = mis_claim(st4, wv, wb);
+          if (__shfl_sync(kFull, claimed, 0)) {
+            for (int i = wbeg + lane; i < wend; i += 32) {
+              const int u = __ldg(&nlist[i]);
+              if ((unsigned)u < (unsigned)n) mis_set_out(st4, u);
+            }
+          }
+        } else if (wverdict == kOut && lane == 0) {
+          mis_set_out(st4, wv);
+        }
+        if (lane == who) verdict = wverdict;
+      }
+      if (und && verdict == kWait) missing = true;
+    }
+    if (!__any_sync(kFull, missing)) break;
+    if (sweep >= max_sweeps) {
+      if (lane == 0) raise(status, ECL_ERR_NO_CONVERGENCE, warp);
+      break;
+    }
+  }
+  if (lane == 0) fetch_max(&status->rounds, sweep + 1);
+}
+
+__global__ void __launch_bounds__(kTPB) mis_emit(int n, const unsigned* __restrict__ st4,
+                                                 unsigned char* __restrict__ out) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    out[v] = (unsigned char)byte_of(st4[v >> 2], v);
+  }
+}
+
+void mis_layout(Carve& c, int n, unsigned** st4) { *st4 = c.take<unsigned>((size_t)(n + 3) / 4); }
+
+}  // namespace
+
+size_t mis_workspace_bytes(int n, int m) {
+  (void)m;
+  Carve c;
+  unsigned* st4;
+  mis_layout(c, n, &st4);
+  return c.bytes();
+}
+
+}  // namespace ecl
+
+extern "C" ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status_out, ecl_opts* opts) {
+  using namespace ecl;
+  ecl_opts local{};
+  if (!opts) opts = &local;
+  if (!status_out) return ECL_ERR_INVALID_ARG;
+  Solve s(g, opts);
+  GraphNeeds needs;
+  needs.symmetric = true;
+  needs.no_self_loops = true;
+  ecl_status st = s.begin(needs, g ? mis_workspace_bytes(g->nodes, g->edges) : 0);
+  if (st != ECL_OK) return s.finish(st);
+  unsigned char* out = s.output(status_out, (size_t)s.n);
+  if (!out) return s.finish(ECL_ERR_OOM);
+  Carve c{s.ws};
+  unsigned* st4;
+  mis_layout(c, s.n, &st4);
+  const int nwords = (s.n + 3) / 4;
+  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
+  // Each sweep decides at least the top-priority undecided vertex, so n + 1
+  // sweeps always suffice for a valid graph.
+  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : s.n + 1;
+
+  s.start_timer();
+  ECL_LAUNCH(mis_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, st4, nwords, s.status);
+  ECL_LAUNCH(mis_run, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, st4, s.status, max_sweeps);
+  ECL_LAUNCH(mis_emit, grid, kTPB, 0, s.stream, s.n, st4, out);
+  s.stop_timer();
+  return s.finish();
+}
+
+extern "C" ecl_status ecl_compute_mis(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,
+                                      uint8_t* nstat) {
+  ecl_graph_view g{nodes, edges, nidx, nlist, nullptr, ECL_HOST, 0};
+  ecl_opts o{};
+  return ecl_mis(&g, nstat, &o);
+}

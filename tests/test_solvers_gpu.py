@@ -1,0 +1,175 @@
+"""MIS, GC, MST, SCC and APSP on the B200 vs the oracle (bit-exact)."""
+import numpy as np
+import pytest
+
+from conftest import from_edges, undirected
+
+pytestmark = pytest.mark.gpu
+
+
+def sym_cases(ecl):
+    yield "single", ecl.Graph(np.array([0, 0], np.int32), np.array([], np.int32), symmetric=True)
+    yield "pair", undirected(2, [(0, 1)])
+    yield "path", undirected(9, [(i, i + 1) for i in range(8)])
+    yield "star", undirected(300, [(0, i) for i in range(1, 300)])
+    yield "isolated", undirected(12, [(3, 7), (7, 9)])
+    yield "clique", undirected(50, [(i, j) for i in range(50) for j in range(i + 1, 50)])
+    yield "grid", ecl.gen_grid(48, 48, 0.05, seed=1)
+    yield "rmat12", ecl.gen_rmat(12, 16, seed=2)
+    yield "rmat14", ecl.gen_rmat(14, 8, seed=5)
+    yield "er", ecl.gen_er(3000, 0.003, seed=4, symmetrise=True)
+    yield "hub", undirected(9000, [(8999, i) for i in range(8999)] + [(i, i + 1) for i in range(0, 200, 2)])
+
+
+def weighted(g, seed=3, wmax=1 << 20):
+    """Attach pair-symmetric weights to a symmetric graph."""
+    rng = np.random.default_rng(seed)
+    src = np.repeat(np.arange(g.nodes), np.diff(g.nindex))
+    lo = np.minimum(src, g.nlist).astype(np.int64)
+    hi = np.maximum(src, g.nlist).astype(np.int64)
+    key = lo * (g.nodes + 1) + hi
+    uniq, inv = np.unique(key, return_inverse=True)
+    w = rng.integers(1, wmax, size=uniq.shape[0]).astype(np.int32)
+    g.eweight = w[inv]
+    return g
+
+
+# ------------------------------------------------------------------------- MIS
+
+
+def test_mis_matches_oracle(ecl, orc):
+    for name, g in sym_cases(ecl):
+        got = ecl.mis(g)
+        assert np.array_equal(got, orc.mis(g)), name
+        assert orc.verify_mis(g, got) == 0, name
+
+
+def test_mis_device_resident(ecl, orc):
+    g = ecl.gen_rmat(14, 16, seed=2)
+    out = ecl.mis(g.to_device())
+    assert np.array_equal(out.cpu().numpy(), orc.mis(g))
+
+
+def test_mis_self_loop_reports_no_convergence(ecl):
+    """The reference spins forever on a self-loop (v never beats itself);
+    here the sweep cap returns ECL_ERR_NO_CONVERGENCE."""
+    g = from_edges(3, [(0, 0), (0, 1), (1, 0)])
+    with pytest.raises(ecl.EclError) as e:
+        ecl.mis(g, max_rounds=50)
+    assert e.value.status == ecl.ERR_NO_CONVERGENCE
+    with pytest.raises(ecl.EclError) as e:
+        ecl.mis(g, validate=True)
+    assert e.value.status == ecl.ERR_BAD_GRAPH
+
+
+# -------------------------------------------------------------------------- GC
+
+
+def test_gc_matches_greedy_oracle(ecl, orc):
+    for name, g in sym_cases(ecl):
+        got = ecl.gc(g)
+        exp = orc.gc(g)
+        assert orc.verify_gc(g, got)[0] == 0, name
+        assert np.array_equal(got, exp), name
+
+
+def test_gc_large_colour_windows(ecl, orc):
+    # a 150-clique forces colours far beyond one 64-colour window
+    g = undirected(160, [(i, j) for i in range(150) for j in range(i + 1, 150)] + [(150 + k, k) for k in range(10)])
+    got = ecl.gc(g)
+    assert np.array_equal(got, orc.gc(g))
+    assert got.max() == 149
+
+
+# ------------------------------------------------------------------------- MST
+
+
+def test_mst_matches_kruskal(ecl, orc):
+    for name, g in sym_cases(ecl):
+        g = weighted(g)
+        inm, tot = ecl.mst(g)
+        einm, etot = orc.mst(g)
+        assert tot == etot, name
+        assert np.array_equal(inm, einm), name
+
+
+def test_mst_ties_broken_by_edge_index(ecl, orc):
+    g = ecl.gen_grid(40, 40, 0.0, seed=1)
+    g.eweight = np.ones(g.edges, np.int32)  # all weights equal: (w, j) order decides
+    inm, tot = ecl.mst(g)
+    einm, etot = orc.mst(g)
+    assert tot == etot == g.nodes - 1
+    assert np.array_equal(inm, einm)
+
+
+def test_mst_generated_weights_and_filter(ecl, orc):
+    # avg degree >= 4 takes the light/heavy path
+    g = ecl.gen_rmat(14, 16, seed=2, weight_seed=3, weight_max=1 << 20)
+    for sym in (False, True):
+        g.symmetric = sym
+        inm, tot = ecl.mst(g)
+        einm, etot = orc.mst(g)
+        assert tot == etot and np.array_equal(inm, einm)
+
+
+# ------------------------------------------------------------------------- SCC
+
+
+def dir_cases(ecl):
+    yield "cycle", from_edges(5, [(0, 1), (1, 2), (2, 0), (3, 4)])
+    yield "two_cycles", from_edges(8, [(0, 1), (1, 0), (1, 2), (2, 3), (3, 4), (4, 2), (5, 6), (6, 7), (7, 5), (4, 5)])
+    yield "self", from_edges(3, [(0, 0), (1, 2), (2, 1), (2, 2)])
+    yield "dag", from_edges(6, [(0, 1), (1, 2), (2, 3), (3, 4), (4, 5), (0, 5)])
+    yield "rmat12d", ecl.gen_rmat(12, 16, seed=2, symmetrise=False)
+    yield "rmat15d", ecl.gen_rmat(15, 8, seed=7, symmetrise=False)
+    yield "er_d", ecl.gen_er(4000, 0.0008, seed=4)
+    yield "sym", ecl.gen_rmat(11, 8, seed=3)
+
+
+def test_scc_matches_tarjan(ecl, orc):
+    for name, g in dir_cases(ecl):
+        got = ecl.scc(g)
+        assert np.array_equal(got, orc.scc(g)), name
+
+
+# ------------------------------------------------------------------------ APSP
+
+
+def apsp_cases(ecl):
+    yield "tiny", from_edges(3, [(0, 1), (1, 2), (0, 2), (0, 2)], weights=[2, 3, 9, 7])
+    yield "selfloop", from_edges(2, [(0, 0), (0, 1)], weights=[4, 1])
+    yield "er200", ecl.gen_er(200, 0.02, seed=4, weight_seed=5)
+    yield "er300", ecl.gen_er(300, 0.01, seed=9, weight_seed=6)
+    yield "er512", ecl.gen_er(512, 0.004, seed=4, weight_seed=4)
+
+
+def test_apsp_matches_fw(ecl, orc):
+    for name, g in apsp_cases(ecl):
+        got = ecl.apsp(g)
+        assert np.array_equal(got, orc.apsp(g)), name
+
+
+def test_apsp_leading_dimension_and_device(ecl, orc):
+    import torch
+
+    g = ecl.gen_er(256, 0.01, seed=11, weight_seed=12)
+    exp = orc.apsp(g)
+    out = np.full((256, 300), -7, np.int32)
+    ecl.apsp(g, out=out, ld=300)
+    assert np.array_equal(out[:, :256], exp) and np.all(out[:, 256:] == -7)
+    d = ecl.apsp(g.to_device())  # n % 128 == 0, ld == n: computed in place
+    assert np.array_equal(d.cpu().numpy(), exp)
+
+
+def test_apsp_reference_padded_layout(ecl, orc):
+    import ctypes as C
+
+    g = ecl.gen_er(100, 0.03, seed=13, weight_seed=14)
+    upper = 128
+    out = np.zeros((upper, upper), np.int32)
+    st = ecl.lib.ecl_compute_apsp(g.nodes, g.edges, g.nindex.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  g.nlist.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  g.eweight.ctypes.data_as(C.POINTER(C.c_int32)), out.ctypes.data_as(C.POINTER(C.c_int32)))
+    assert st == 0
+    assert np.array_equal(out[:100, :100], orc.apsp(g))
+    assert np.all(out[100:, :] == ecl.APSP_INF) and np.all(out[:, 100:] == ecl.APSP_INF)
