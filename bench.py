@@ -1,0 +1,533 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 race-free graph suite (the driver's contract).
+
+Default workload (one "step"): the full plain suite on R-MAT scale 22
+(2^22 vertices, edge factor 16, a=.57 b=.19 c=.19, seed 2): CC, MIS, GC and
+MST (int32 weights uniform in [1, 2^20), seed 3, symmetric per pair) on the
+symmetrised, duplicate- and self-loop-free graph, and SCC on the directed
+graph of the same parameters.  Metric: edges/s = sum of each solve's
+g.edges / sum of solve times, as the reference computes edges/s
+(ECL-CC-atomic.cu:314-316): inputs resident on the device, kernel time only.
+L2 (126 MB) is flushed by a 256 MiB write before every solve.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload suite|grid|apsp] [--scale S]
+
+Multi-GPU: replicas only -- every rank solves its own copy of the workload, no
+collective on the data path; value = edges of all ranks / max time over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ecl-suite_b200"))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+CODES_SYM = ["cc", "mis", "gc", "mst"]
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["suite", "grid", "apsp"], default="suite")
+    p.add_argument("--scale", type=int, default=22)
+    p.add_argument("--e2e-steps", type=int, default=2)
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        d["source"] = "measured"
+        return d
+    except Exception:
+        return dict(PEAKS_FALLBACK)
+
+
+# ---------------------------------------------------------------- clocks
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- workloads
+
+
+def make_suite_graphs(ecl, scale):
+    sym = ecl.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=True, weight_seed=3, weight_max=1 << 20)
+    dirg = ecl.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=False)
+    return sym, dirg
+
+
+# Algorithmic (compulsory) bytes of each kernel phase, per launch: the bytes
+# the phase must move at minimum (CSR read once, per-vertex state read or
+# written once).  n = vertices, m = CSR entries.
+def phase_bytes(code, phase, n, m):
+    csr = 4 * (n + 1) + 4 * m
+    table = {
+        ("cc", 0): 4 * (n + 1) + 4 * n,            # init: nindex + first entries, parent write
+        ("cc", 1): csr + 4 * n,                    # hook: CSR + parent
+        ("cc", 2): 4 * m // 8,                     # chunks: hub entries (upper bound share)
+        ("cc", 3): 8 * n,                          # flatten: parent read + write
+        ("mis", 0): 4 * (n + 1) + n,
+        ("mis", 1): csr + n,
+        ("mis", 2): 2 * n,
+        ("gc", 0): csr + 4 * (m // 2) + 12 * n,    # init: CSR + higher-priority list + state
+        ("gc", 1): 4 * (m // 2) + 12 * n,          # run: higher-priority lists + state + colour
+        ("mst", 0): 16 * n,
+        ("mst", 1): 4 * (n + 1) + 8 * m,           # light scan: CSR + weights
+        ("mst", 2): 16 * n,
+        ("mst", 3): 4 * (n + 1) + 8 * m + 4 * n,   # heavy scan: CSR + weights + roots
+        ("mst", 4): 16 * n,
+        ("scc", 0): csr + 12 * n,
+        ("scc", 1): csr + 4 * n,
+        ("scc", 2): 8 * m + 12 * n,
+    }
+    return table.get((code, phase), csr)
+
+
+PHASE_NAMES = {
+    "cc": ["cc_init", "cc_hook", "cc_chunks", "cc_flatten"],
+    "mis": ["mis_init", "mis_run", "mis_emit"],
+    "gc": ["gc_init", "gc_run"],
+    "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
+            "mst_boruvka(heavy)"],
+    "scc": ["scc_mark", "scc_build", "scc_solve"],
+    "apsp": ["apsp_fill+edges", "apsp_panels+update"],
+}
+
+
+# ---------------------------------------------------------------- our arm
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import ecl_b200 as ecl
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+
+    if args.workload == "suite":
+        sym, dirg = make_suite_graphs(ecl, args.scale)
+        jobs = [(c, sym) for c in CODES_SYM] + [("scc", dirg)]
+        wl_name = (f"rmat{args.scale}-suite: CC+MIS+GC+MST on symmetrised R-MAT-{args.scale} "
+                   f"(n={sym.nodes}, m={sym.edges}), SCC on directed R-MAT-{args.scale} (m={dirg.edges})")
+    elif args.workload == "grid":
+        g = ecl.gen_grid(1024, 1024, 0.05, seed=1)
+        jobs = [("cc", g)]
+        wl_name = f"grid1024-cc: CC on 1024x1024 grid, 5% deleted (n={g.nodes}, m={g.edges})"
+    else:
+        g = ecl.gen_er(8192, 0.001, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+        jobs = [("apsp", g)]
+        wl_name = f"er8192-apsp: blocked FW on ER n=8192 p=0.001 (m={g.edges})"
+
+    dgs = {}
+    for code, g in jobs:
+        if id(g) not in dgs:
+            dgs[id(g)] = g.to_device(dev)
+    wsb = max(ecl.workspace_bytes(getattr(ecl, code.upper()), g.nodes, g.edges) for code, g in jobs)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=dev)
+    outs = {}
+    for code, g in jobs:
+        if code == "mst":
+            outs[code] = torch.empty(max(g.edges, 1), dtype=torch.uint8, device=dev)
+        elif code == "mis":
+            outs[code] = torch.empty(g.nodes, dtype=torch.uint8, device=dev)
+        elif code == "apsp":
+            outs[code] = torch.empty((g.nodes, g.nodes), dtype=torch.int32, device=dev)
+        else:
+            outs[code] = torch.empty(g.nodes, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def solve(code, g, detail):
+        o = ecl._opts(stream=sh, workspace=ws, detail=detail)
+        dg = dgs[id(g)]
+        fn = getattr(ecl, code)
+        if code == "apsp":
+            fn(dg, out=outs[code], opts=o)
+        else:
+            fn(dg, out=outs[code], opts=o)
+        return o
+
+    per_code_ms = {c: 0.0 for c, _ in jobs}
+    phase_tot = {}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    def step(timed):
+        tot = 0.0
+        for code, g in jobs:
+            flush.fill_(1)
+            ev0.record(stream)
+            o = solve(code, g, detail=timed)
+            ev1.record(stream)
+            ev1.synchronize()
+            ms = ev0.elapsed_time(ev1)
+            if timed:
+                per_code_ms[code] += ms
+                for i in range(o.nphases):
+                    key = (code, i)
+                    phase_tot[key] = phase_tot.get(key, 0.0) + o.phase_ms[i]
+            tot += ms
+        return tot
+
+    for _ in range(args.warmup):
+        step(False)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local_rank)
+    clk.start()
+    l0 = ecl.kernel_launches()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        total_ms += step(True)
+    launches = ecl.kernel_launches() - l0
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = clk.stop()
+
+    edges_step = sum(g.edges for _, g in jobs)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * edges_step * args.steps / (total_ms / 1e3)
+    ms_per_step = total_ms / args.steps
+
+    # dominant kernel phase and its roofline
+    dom = max(phase_tot.items(), key=lambda kv: kv[1]) if phase_tot else None
+    pk = peaks()
+    roof = None
+    if dom is not None and jobs[0][0] != "apsp":
+        (code, idx), tot = dom
+        g = dict(jobs)[code]
+        avg_ms = tot / args.steps
+        byts = phase_bytes(code, idx, g.nodes, g.edges)
+        ach = byts / (avg_ms / 1e3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+                traffic = json.load(f).get(PHASE_NAMES[code][idx])
+        except Exception:
+            pass
+        roof = {"bound": "hbm", "kernel": PHASE_NAMES[code][idx], "achieved": round(ach, 1),
+                "peak": pk.get("hbm_gbs"), "unit": "GB/s", "frac": round(ach / pk.get("hbm_gbs", 1), 4),
+                "traffic": traffic, "algorithmic_bytes": byts, "avg_ms": round(avg_ms, 4),
+                "share": round(tot / sum(phase_tot.values()), 3), "peak_source": pk.get("source")}
+    elif dom is not None:
+        (code, idx), tot = dom
+        g = dict(jobs)[code]
+        n = g.nodes
+        avg_ms = tot / args.steps
+        ops = 2.0 * n ** 3  # one add + one min per update
+        roof = {"bound": "int32", "kernel": "apsp_panels+apsp_update", "achieved": round(ops / (avg_ms / 1e3) / 1e12, 3),
+                "peak": None, "unit": "Tops/s", "frac": None, "traffic": None, "avg_ms": round(avg_ms, 3),
+                "note": "INT32 add+min (2 ops per update; one DPX viaddmin instruction)"}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        hosts = {}
+
+        def pinned(a):
+            t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+            return t.numpy(), t
+
+        keep = []
+        for code, g in jobs:
+            if id(g) in hosts:
+                continue
+            ni, t1 = pinned(g.nindex)
+            nl, t2 = pinned(g.nlist)
+            ew = None
+            if g.eweight is not None:
+                ew, t3 = pinned(g.eweight)
+                keep.append(t3)
+            keep += [t1, t2]
+            hosts[id(g)] = ecl.Graph(ni, nl, ew, g.symmetric)
+        houts = {}
+        for code, g in jobs:
+            if code == "apsp":
+                t = torch.empty((g.nodes, g.nodes), dtype=torch.int32).pin_memory()
+            elif code in ("mst",):
+                t = torch.empty(max(g.edges, 1), dtype=torch.uint8).pin_memory()
+            elif code == "mis":
+                t = torch.empty(g.nodes, dtype=torch.uint8).pin_memory()
+            else:
+                t = torch.empty(g.nodes, dtype=torch.int32).pin_memory()
+            keep.append(t)
+            houts[code] = t.numpy()
+        h2d = d2h = 0
+        for code, g in jobs:
+            h2d += 4 * (g.nodes + 1) + 4 * g.edges + (4 * g.edges if code in ("mst", "apsp") else 0)
+            d2h += houts[code].nbytes if code != "mst" else g.edges
+        e_ms = 0.0
+        for it in range(args.e2e_steps + 1):
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            for code, g in jobs:
+                o = ecl._opts(stream=sh)
+                fn = getattr(ecl, code)
+                fn(hosts[id(g)], out=houts[code], opts=o)
+            ev1.record(stream)
+            ev1.synchronize()
+            if it > 0:  # first call warms the stream-ordered allocator
+                e_ms += ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([e_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": world * edges_step * args.e2e_steps / (e_ms / 1e3), "unit": "edges/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
+               "ms_per_step": e_ms / args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and args.workload == "suite":
+        cpu = cpu_baseline(ecl, scale=min(args.scale, 21))
+
+    per_code = {c: {"edges": g.edges, "ms": per_code_ms[c] / args.steps,
+                    "edges_per_s": g.edges / (per_code_ms[c] / args.steps / 1e3)} for c, g in jobs}
+    phases = {f"{PHASE_NAMES[c][i]}": round(v / args.steps, 4) for (c, i), v in sorted(phase_tot.items())}
+    line = {
+        "metric": "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)",
+        "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded generators: R-MAT / grid / Erdos-Renyi)",
+        "config": {"workload": wl_name, "l2": "256 MiB write before every solve; CSR 513 MB > L2",
+                   "parallelism": f"replicas x{world}"},
+        "per_code": per_code, "phase_ms": phases, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- CPU baseline / reference arm
+
+
+def _orc():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return oracle
+
+
+def _ref():
+    p = os.path.join(ROOT, "oracle", "_ref", "libeclref.so")
+    if not os.path.exists(p):
+        return None
+    r = C.CDLL(p)
+    r.eclref_mst_cpu.restype = C.c_double
+    r.eclref_mst_gpu.restype = C.c_double
+    r.eclref_cc_device.restype = C.c_float
+    r.eclref_mis_device.restype = C.c_float
+    r.eclref_gc_device.restype = C.c_float
+    r.eclref_gc_scratch_bytes.restype = C.c_size_t
+    r.eclref_scc_device.restype = C.c_float
+    r.eclref_scc_scratch_bytes.restype = C.c_size_t
+    return r
+
+
+def cpu_suite_once(ecl, sym, dirg, orc, ref):
+    """One pass of the CPU suite: serial oracle ports of CC/MIS/GC/SCC (the
+    reference has no CPU solver for them) and the reference's own serial
+    cpuMST (ECL-MST_10-atomic.cu:112) when oracle/_ref is built.
+    Returns (edges, seconds, kinds)."""
+    import numpy as np
+
+    t_total, e_total, kinds = 0.0, 0, {}
+    for code in ("cc", "mis", "gc"):
+        t0 = time.perf_counter()
+        getattr(orc, code)(sym)
+        t_total += time.perf_counter() - t0
+        e_total += sym.edges
+        kinds[code] = "port"
+    out = np.zeros(sym.edges, np.uint8)
+    t0 = time.perf_counter()
+    if ref is not None:
+        P = lambda a: C.c_void_p(a.ctypes.data)
+        ref.eclref_mst_cpu(sym.nodes, sym.edges, P(sym.nindex), P(sym.nlist), P(sym.eweight), P(out))
+        kinds["mst"] = "reference"
+    else:
+        orc.mst(sym)
+        kinds["mst"] = "port"
+    t_total += time.perf_counter() - t0
+    e_total += sym.edges
+    t0 = time.perf_counter()
+    orc.scc(dirg)
+    t_total += time.perf_counter() - t0
+    e_total += dirg.edges
+    kinds["scc"] = "port"
+    return e_total, t_total, kinds
+
+
+def cpu_baseline(ecl, scale):
+    orc = _orc()
+    ref = _ref()
+    sym, dirg = make_suite_graphs(ecl, scale)
+    e, t, kinds = cpu_suite_once(ecl, sym, dirg, orc, ref)
+    return {"value": e / t, "unit": "edges/s", "cores": 1,
+            "kind": "reference" if kinds.get("mst") == "reference" else "port",
+            "sample": f"one serial pass of the suite on R-MAT-{scale} (same generator parameters): "
+                      f"CC/MIS/GC/SCC by the C oracle port, MST by the reference's own cpuMST; {t:.1f} s",
+            "per_code_kind": kinds}
+
+
+def reference_gpu(ecl, sym, dirg):
+    """The reference's race-free CUDA build (oracle/_ref) on the same graphs:
+    kernel time as each reference driver times it."""
+    import numpy as np
+    import torch
+
+    ref = _ref()
+    if ref is None or not torch.cuda.is_available():
+        return None
+    P = lambda t: C.c_void_p(t.data_ptr())
+    ni, nl = torch.from_numpy(sym.nindex).cuda(), torch.from_numpy(sym.nlist).cuda()
+    res = {}
+    st = torch.empty(sym.nodes, dtype=torch.int32, device="cuda")
+    wl = torch.empty(sym.nodes, dtype=torch.int32, device="cuda")
+    res["cc"] = min(ref.eclref_cc_device(sym.nodes, P(ni), P(nl), P(st), P(wl)) for _ in range(3))
+    st8 = torch.empty((sym.nodes + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
+    res["mis"] = min(ref.eclref_mis_device(sym.nodes, sym.edges, P(ni), P(nl), P(st8)) for _ in range(3))
+    scr = torch.empty(ref.eclref_gc_scratch_bytes(sym.nodes, sym.edges) // 4 + 1, dtype=torch.int32, device="cuda")
+    res["gc"] = min(ref.eclref_gc_device(sym.nodes, sym.edges, P(ni), P(nl), P(st), P(scr)) for _ in range(3))
+    del scr
+    inm = np.zeros(sym.edges, np.uint8)
+    Q = lambda a: C.c_void_p(a.ctypes.data)
+    res["mst"] = min(ref.eclref_mst_gpu(sym.nodes, sym.edges, Q(sym.nindex), Q(sym.nlist), Q(sym.eweight), Q(inm))
+                     for _ in range(2))
+    del ni, nl, st, wl, st8
+    di, dl = torch.from_numpy(dirg.nindex).cuda(), torch.from_numpy(dirg.nlist).cuda()
+    scr = torch.empty(ref.eclref_scc_scratch_bytes(dirg.nodes, dirg.edges) // 8 + 2, dtype=torch.int64, device="cuda")
+    res["scc"] = min(ref.eclref_scc_device(dirg.nodes, dirg.edges, P(di), P(dl), None, P(scr)) for _ in range(2))
+    edges = {"cc": sym.edges, "mis": sym.edges, "gc": sym.edges, "mst": sym.edges, "scc": dirg.edges}
+    tot_e = sum(edges.values())
+    tot_ms = sum(res.values())
+    return {"value": tot_e / (tot_ms / 1e3), "unit": "edges/s",
+            "per_code": {c: {"ms": res[c], "edges_per_s": edges[c] / (res[c] / 1e3)} for c in res},
+            "note": "reference race-free CUDA build (nvcc -O3 sm_100a), same graphs, its own timed regions"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import ecl_b200 as ecl
+
+    orc = _orc()
+    ref = _ref()
+    scale = min(args.scale, 20)  # a bounded sample of the workload for the serial CPU codes
+    sym, dirg = make_suite_graphs(ecl, scale)
+    for _ in range(min(args.warmup, 1)):
+        cpu_suite_once(ecl, sym, dirg, orc, ref)
+    e_tot, t_tot, kinds = 0, 0.0, {}
+    for _ in range(args.steps):
+        e, t, kinds = cpu_suite_once(ecl, sym, dirg, orc, ref)
+        e_tot += e
+        t_tot += t
+    value = e_tot / t_tot
+    gpu = None
+    try:
+        big_sym, big_dir = make_suite_graphs(ecl, args.scale)
+        gpu = reference_gpu(ecl, big_sym, big_dir)
+    except Exception as ex:  # reported, not fatal: the CPU arm is the reference arm
+        gpu = {"error": str(ex)}
+    line = {
+        "impl": "reference",
+        "metric": "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)",
+        "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t_tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded generators)",
+        "config": {"workload": f"rmat{args.scale}-suite (CPU sample: R-MAT-{scale})", "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1,
+                         "kind": "reference" if kinds.get("mst") == "reference" else "port",
+                         "sample": f"serial suite on R-MAT-{scale}: MST = reference cpuMST, CC/MIS/GC/SCC = C oracle port",
+                         "per_code_kind": kinds},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import datetime
+
+    import torch
+
+    if world > 1:
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

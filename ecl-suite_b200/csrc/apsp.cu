@@ -310,11 +310,13 @@ extern "C" ecl_status ecl_apsp(const ecl_graph_view* g, int32_t* dist, int64_t l
   s.start_timer();
   ECL_LAUNCH(apsp_fill, grid, 256, 0, s.stream, W, (long)N, N, s.n);
   if (s.m > 0) ECL_LAUNCH(apsp_edges, (s.n + 255) / 256, 256, 0, s.stream, W, (long)N, s.n, s.m, s.nindex, s.nlist, s.eweight, s.status);
+  s.mark();
   for (int kb = 0; kb < nb; kb++) {
     ECL_LAUNCH(apsp_panels, 1 + 2 * (nb - 1), kThreads, kPanelSmem, s.stream, W, (long)N, nb, kb, Dbuf);
     if (nb > 1)
       ECL_LAUNCH(apsp_update, (nb - 1) * (nb - 1) + 1, kThreads, kUpdateSmem, s.stream, W, (long)N, nb, kb, Dbuf);
   }
+  s.mark();
   s.stop_timer();
   if (!inplace) {
     const cudaMemcpyKind kind = g->location == ECL_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;

@@ -224,9 +224,13 @@ extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* 
   s.start_timer();
   if (cudaMemsetAsync(ctr, 0, sizeof(CCCounters), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
   ECL_LAUNCH(cc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, s.status);
+  s.mark();
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, chunks, ctr, s.status);
+  s.mark();
   ECL_LAUNCH(cc_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, parent, chunks, ctr, s.status);
+  s.mark();
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, s.stream, s.n, parent);
+  s.mark();
   s.stop_timer();
   return s.finish();
 }

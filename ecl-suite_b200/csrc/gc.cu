@@ -247,7 +247,9 @@ extern "C" ecl_status ecl_gc(const ecl_graph_view* g, int32_t* color_out, ecl_op
 
   s.start_timer();
   ECL_LAUNCH(gc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, hl, hc, state, color, s.status);
+  s.mark();
   ECL_LAUNCH(gc_run, grid, kTPB, 0, s.stream, s.n, s.nindex, hl, hc, state, color, s.status, max_sweeps);
+  s.mark();
   s.stop_timer();
   return s.finish();
 }

@@ -19,8 +19,9 @@
 //    32 entries per step by the whole warp (two ballots per step); a joining
 //    vertex claims itself with one CAS, then clears its neighbours' bytes
 //    (fetch_and), so blocked neighbours see OUT without rescanning;
-//  * a sweep cap turns a non-converging input (self-loop, asymmetric list --
-//    the reference spins forever there) into ECL_ERR_NO_CONVERGENCE.
+//  * a self-loop (the reference spins forever on one: v never outranks
+//    itself) raises ECL_ERR_BAD_GRAPH when it is met; a sweep cap turns any
+//    other non-converging input into ECL_ERR_NO_CONVERGENCE.
 #include "runtime.cuh"
 
 namespace ecl {
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
         verdict = kJoin;
         for (int i = beg; i < end; i++) {
           const int u = __ldg(&nlist[i]);
-          if ((unsigned)u >= (unsigned)n) {
+          if ((unsigned)u >= (unsigned)n || u == v) {  // out of range, or a self-loop
             raise(status, ECL_ERR_BAD_GRAPH, u);
             continue;
           }
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
           int r = kJoin;
           if (i < wend) {
             const int u = __ldg(&nlist[i]);
-            if ((unsigned)u < (unsigned)n) {
+            if ((unsigned)u < (unsigned)n && u != wv) {
               r = mis_verdict(byte_of(ld(&st4[u >> 2]), u), wb, u, wv);
             } else {
               raise(status, ECL_ERR_BAD_GRAPH, u);
@@ -238,8 +239,11 @@ extern "C" ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status_out, ecl_
 
   s.start_timer();
   ECL_LAUNCH(mis_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, st4, nwords, s.status);
+  s.mark();
   ECL_LAUNCH(mis_run, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, st4, s.status, max_sweeps);
+  s.mark();
   ECL_LAUNCH(mis_emit, grid, kTPB, 0, s.stream, s.n, st4, out);
+  s.mark();
   s.stop_timer();
   return s.finish();
 }

@@ -389,6 +389,7 @@ extern "C" ecl_status ecl_mst(const ecl_graph_view* g, uint8_t* in_mst_out, uint
   ECL_LAUNCH(mst_init, grid, kTPB, 0, s.stream, s.n, b.parent, b.minv);
   if (s.m > 0) {
     ECL_LAUNCH(mst_threshold, 1, kSamples, 0, s.stream, s.n, s.m, s.eweight, b.ctl);
+    s.mark();
     for (int pass = 0; pass < 2; pass++) {
       if (pass == 0) {
         ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
@@ -401,12 +402,14 @@ extern "C" ecl_status ecl_mst(const ecl_graph_view* g, uint8_t* in_mst_out, uint
         ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, s.status);
       }
+      s.mark();
       int n_ = s.n;
       int pass_ = pass;
       void* args[] = {&n_, &pass_, &b.wlA, &b.wlB, &b.parent, &b.minv, &in_mst, &b.ctl, &s.status};
       if (cudaLaunchCooperativeKernel((void*)mst_boruvka, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
         return s.finish(ECL_ERR_CUDA);
       count_launch();
+      s.mark();
       // The heavy pass (pass 1) runs unconditionally: with no filter it finds
       // no entry above the INT_MAX threshold and ends after one round.
     }

@@ -146,6 +146,14 @@ void Solve::start_timer() {
   cudaEventRecord(ev0_, stream);
 }
 
+void Solve::mark() {
+  if (!opts_ || !opts_->detail || marks_.size() >= 8) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, stream);
+  marks_.push_back(e);
+}
+
 void Solve::stop_timer() {
   cudaEventRecord(ev1_, stream);
   timed_ = true;
@@ -177,11 +185,22 @@ ecl_status Solve::finish(ecl_status st) {
   if (opts_) {
     opts_->rounds = hs.rounds;
     opts_->elapsed_ms = 0.f;
+    opts_->nphases = 0;
     if (timed_ && e == cudaSuccess) {
       float ms = 0.f;
       if (cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess) opts_->elapsed_ms = ms;
+      cudaEvent_t prev = ev0_;
+      for (size_t i = 0; i < marks_.size(); i++) {
+        float pm = 0.f;
+        cudaEventElapsedTime(&pm, prev, marks_[i]);
+        opts_->phase_ms[i] = pm;
+        prev = marks_[i];
+      }
+      opts_->nphases = (int32_t)marks_.size();
     }
   }
+  for (cudaEvent_t m : marks_) cudaEventDestroy(m);
+  marks_.clear();
   for (void* p : temps_) cudaFreeAsync(p, stream);
   temps_.clear();
   outs_.clear();

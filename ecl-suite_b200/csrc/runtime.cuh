@@ -94,6 +94,8 @@ class Solve {
   void* temp(size_t bytes);
 
   void start_timer();
+  // Ends a kernel phase (only recorded when opts->detail is set).
+  void mark();
   void stop_timer();
   // Copies outputs back, synchronises, folds the device status into the
   // return code and releases temporaries.
@@ -121,6 +123,7 @@ class Solve {
   std::vector<Copy> outs_;
   std::vector<void*> temps_;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  std::vector<cudaEvent_t> marks_;
   bool timed_ = false;
   bool finished_ = false;
 };

@@ -300,12 +300,15 @@ extern "C" ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label_out, ecl_o
     return s.finish(ECL_ERR_CUDA);
   if (cudaMemsetAsync(b.hasin, 0, sizeof(int) * (size_t)s.n, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
   ECL_LAUNCH(scc_mark, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.imax, b.omax, s.status);
+  s.mark();
   ECL_LAUNCH(scc_build, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.wlA, b.ctl);
+  s.mark();
   int n_ = s.n;
   void* args[] = {&n_, &b.wlA, &b.wlB, &b.imax, &b.omax, &label, &b.ctl, &b.rounds, &max_rounds, &s.status};
   if (cudaLaunchCooperativeKernel((void*)scc_solve, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
     return s.finish(ECL_ERR_CUDA);
   count_launch();
+  s.mark();
   s.stop_timer();
   return s.finish();
 }

@@ -68,6 +68,9 @@ class Opts(C.Structure):
         ("max_rounds", C.c_int32),
         ("elapsed_ms", C.c_float),
         ("rounds", C.c_int32),
+        ("detail", C.c_int32),
+        ("nphases", C.c_int32),
+        ("phase_ms", C.c_float * 8),
     ]
 
 
@@ -260,9 +263,10 @@ class DeviceGraph:
 # ---- solvers ---------------------------------------------------------------------
 
 
-def _opts(stream=None, workspace=None, validate=False, max_rounds=0) -> Opts:
+def _opts(stream=None, workspace=None, validate=False, max_rounds=0, detail=False) -> Opts:
     o = Opts()
     o.stream = stream
+    o.detail = int(detail)
     if workspace is not None:
         o.workspace = workspace.data_ptr()
         o.workspace_bytes = workspace.numel() * workspace.element_size()

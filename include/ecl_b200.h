@@ -75,6 +75,9 @@ typedef struct ecl_opts {
   int32_t max_rounds;     /* cap on device fixpoint rounds; 0 = built-in default */
   float elapsed_ms;       /* out: device time of the compute phase (CUDA events) */
   int32_t rounds;         /* out: fixpoint rounds / sweeps the solve took */
+  int32_t detail;         /* 1: also time each kernel phase (events between phases) */
+  int32_t nphases;        /* out: number of phase_ms entries written */
+  float phase_ms[8];      /* out: device time of each kernel phase, in launch order */
 } ecl_opts;
 
 /* Solver identifiers (ecl_workspace_bytes). */

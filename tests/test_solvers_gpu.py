@@ -50,13 +50,14 @@ def test_mis_device_resident(ecl, orc):
     assert np.array_equal(out.cpu().numpy(), orc.mis(g))
 
 
-def test_mis_self_loop_reports_no_convergence(ecl):
+def test_mis_self_loop_is_rejected(ecl):
     """The reference spins forever on a self-loop (v never beats itself);
-    here the sweep cap returns ECL_ERR_NO_CONVERGENCE."""
+    here the device scan reports ECL_ERR_BAD_GRAPH, and host validation
+    rejects it before any launch."""
     g = from_edges(3, [(0, 0), (0, 1), (1, 0)])
     with pytest.raises(ecl.EclError) as e:
         ecl.mis(g, max_rounds=50)
-    assert e.value.status == ecl.ERR_NO_CONVERGENCE
+    assert e.value.status == ecl.ERR_BAD_GRAPH
     with pytest.raises(ecl.EclError) as e:
         ecl.mis(g, validate=True)
     assert e.value.status == ecl.ERR_BAD_GRAPH
