@@ -243,7 +243,10 @@ extern "C" ecl_status ecl_gc(const ecl_graph_view* g, int32_t* color_out, ecl_op
   unsigned* state;
   gc_layout(c, s.n, s.m, &hl, &hc, &state);
   const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : s.n + 1;
+  // Warps sweep asynchronously, so one warp may sweep many times while it
+  // waits on a vertex owned by a slower warp: the cap is a fixed backstop
+  // (GC cannot stall -- priorities form a DAG), not a per-graph bound.
+  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : (1 << 22);
 
   s.start_timer();
   ECL_LAUNCH(gc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, hl, hc, state, color, s.status);

@@ -233,9 +233,10 @@ extern "C" ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status_out, ecl_
   mis_layout(c, s.n, &st4);
   const int nwords = (s.n + 3) / 4;
   const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-  // Each sweep decides at least the top-priority undecided vertex, so n + 1
-  // sweeps always suffice for a valid graph.
-  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : s.n + 1;
+  // Warps sweep asynchronously (one may sweep many times while it waits on a
+  // slower warp's vertex), so the cap is a fixed backstop against inputs that
+  // cannot converge, not a per-graph bound.
+  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : (1 << 22);
 
   s.start_timer();
   ECL_LAUNCH(mis_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, st4, nwords, s.status);
