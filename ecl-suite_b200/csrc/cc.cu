@@ -22,6 +22,8 @@
 // All parent accesses are device-scope relaxed atomics; links use CAS.
 #include "runtime.cuh"
 
+#include <mutex>
+
 namespace ecl {
 namespace {
 
@@ -233,6 +235,83 @@ extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* 
   s.mark();
   s.stop_timer();
   return s.finish();
+}
+
+// ---- allocation-free variant --------------------------------------------------
+//
+// ecl_cc_noalloc runs the same four kernels with its scratch (status block,
+// counters, chunk records) in a fixed array that lives in this library's
+// device memory, so the call itself allocates nothing.  Every GPU that loads
+// the library holds the array until the process exits.
+
+namespace ecl {
+namespace {
+
+constexpr size_t kNoAllocBytes = ECL_CC_NOALLOC_SCRATCH_BYTES;
+static_assert(kStatusBytes + sizeof(CCCounters) + 256 + sizeof(int2) * (size_t)(2 * (ECL_CC_NOALLOC_MAX_EDGES / kChunk) + 2) <=
+                  kNoAllocBytes,
+              "no-alloc scratch too small for ECL_CC_NOALLOC_MAX_EDGES");
+
+static __device__ __align__(256) unsigned char g_cc_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+// Device address of g_cc_noalloc_scratch on the current device, looked up
+// once per device (host code cannot use the symbol itself as a pointer).
+ecl_status noalloc_scratch(int device, void** out) {
+  if (device < 0 || device >= 64) return ECL_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_cc_noalloc_scratch);
+    if (e != cudaSuccess) {
+      set_last_error("cudaGetSymbolAddress(g_cc_noalloc_scratch)", e);
+      return ECL_ERR_CUDA;
+    }
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return ECL_OK;
+}
+
+}  // namespace
+}  // namespace ecl
+
+extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t* nindex, const int32_t* nlist,
+                                     int32_t* label, void* stream_ptr) {
+  using namespace ecl;
+  if (nodes < 1 || edges < 0) return ECL_ERR_BAD_GRAPH;
+  if (!nindex || !label || (edges > 0 && !nlist)) return ECL_ERR_INVALID_ARG;
+  if (edges > ECL_CC_NOALLOC_MAX_EDGES) {
+    set_last_error_msg("ecl_cc_noalloc: graph has more CSR entries than ECL_CC_NOALLOC_MAX_EDGES; use ecl_cc");
+    return ECL_ERR_UNSUPPORTED;
+  }
+  DeviceInfo dev;
+  ecl_status st = current_device(&dev);
+  if (st != ECL_OK) return st;
+  void* base = nullptr;
+  st = noalloc_scratch(dev.device, &base);
+  if (st != ECL_OK) return st;
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  Status* status = static_cast<Status*>(base);
+  Carve c{static_cast<char*>(base) + kStatusBytes};
+  CCCounters* ctr;
+  int2* chunks;
+  cc_layout(c, nodes, edges, &ctr, &chunks);
+  // The array keeps the previous call's contents: clear the status block and
+  // the counters (adjacent, at the front of the array) before every solve.
+  ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
+  const int grid = dev.sms * (dev.max_threads_per_sm / kTPB);
+  ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, ctr, status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, ctr, status);
+  ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, nodes, label);
+  Status hs{};
+  ECL_CUDA_TRY(cudaMemcpyAsync(&hs, status, sizeof(hs), cudaMemcpyDeviceToHost, stream));
+  ECL_CUDA_TRY(cudaStreamSynchronize(stream));
+  ECL_CUDA_TRY(cudaGetLastError());
+  return static_cast<ecl_status>(hs.code);
 }
 
 extern "C" ecl_status ecl_compute_cc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,

@@ -151,6 +151,37 @@ ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label, ecl_opts* opts);
  * Requires eweight.  Replaces FW_gpu_64 (ECL-APSP-atomic.cu:460-531). */
 ecl_status ecl_apsp(const ecl_graph_view* g, int32_t* dist, int64_t ld, ecl_opts* opts);
 
+/* ---- allocation-free CC ------------------------------------------------------- */
+
+/* No counterpart in the reference.
+ *
+ * Connected components exactly as ecl_cc computes them, for callers that must
+ * not allocate device memory during a solve: code whose process hands all
+ * device memory to another framework's pool (so cudaMalloc fails or fragments
+ * that pool), code inside an allocator callback or a plugin whose host owns
+ * every allocation, or a latency-critical section where cudaMalloc's implicit
+ * device synchronisation is not acceptable.  The call allocates nothing: the
+ * caller passes the graph and the label array (device pointers of the current
+ * device, same meaning as ecl_cc), and the solver's scratch is a static device
+ * array of ECL_CC_NOALLOC_SCRATCH_BYTES inside this library, which every GPU
+ * that loads the library holds until the process exits.
+ *
+ *  - Graphs with more than ECL_CC_NOALLOC_MAX_EDGES CSR entries are rejected
+ *    with ECL_ERR_UNSUPPORTED (use ecl_cc for those).
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress) with that device current; make that first call
+ *    before any stream capture.
+ *  - All calls share the one array and it keeps the last call's contents (the
+ *    call clears what must start at zero).  Calls that overlap on the GPU --
+ *    different streams, or threads calling at once -- race on it; serialise
+ *    them.
+ *  - Runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ *    synchronises it before returning the status. */
+#define ECL_CC_NOALLOC_MAX_EDGES (1 << 27)
+#define ECL_CC_NOALLOC_SCRATCH_BYTES (2u << 20)
+ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t* nindex, const int32_t* nlist, int32_t* label,
+                          void* stream);
+
 /* ---- reference-shaped wrappers (host pointers, default stream) ---------------- */
 
 /* computeCC(nodes, edges, nidx, nlist, nstat), ECL-CC-atomic.cu:275 */
