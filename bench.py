@@ -124,8 +124,9 @@ def phase_bytes(code, phase, n, m):
         ("mis", 0): 4 * (n + 1) + n,
         ("mis", 1): csr + n,
         ("mis", 2): 2 * n,
-        ("gc", 0): csr + 4 * (m // 2) + 12 * n,    # init: CSR + higher-priority list + state
-        ("gc", 1): 4 * (m // 2) + 12 * n,          # run: higher-priority lists + state + colour
+        ("gc", 0): csr + 4 * (m // 2) + 4 * n,     # init: CSR read, higher-priority half of nl2 + counts written
+        ("gc", 1): 7 * 24 * n,                     # keys + 7 radix passes over (8 B key, 4 B value), read + write
+        ("gc", 2): 4 * (n + 1) + 4 * (m // 2) + 12 * n,  # pull: higher-priority half read once, order, colours
         ("mst", 0): 16 * n,
         ("mst", 1): 4 * (n + 1) + 8 * m,           # light scan: CSR + weights
         ("mst", 2): 16 * n,
@@ -141,10 +142,10 @@ def phase_bytes(code, phase, n, m):
 PHASE_NAMES = {
     "cc": ["cc_init", "cc_hook", "cc_chunks", "cc_flatten"],
     "mis": ["mis_init", "mis_run", "mis_emit"],
-    "gc": ["gc_init", "gc_run"],
+    "gc": ["gc_init+chunks", "gc_keys+radix_sort", "gc_pull"],
     "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
             "mst_boruvka(heavy)"],
-    "scc": ["scc_mark", "scc_build", "scc_solve"],
+    "scc": ["scc_mark+chunks", "scc_build+chunks", "scc_solve"],
     "apsp": ["apsp_fill+edges", "apsp_panels+update"],
 }
 

@@ -9,7 +9,8 @@
 // so any union-find with the same hooking rule reproduces it bit for bit.
 //
 // B200 design:
-//  * cc_init   - parent[v] = first smaller neighbour (one free hook per vertex).
+//  * cc_init   - parent[v] = first smaller neighbour among the first
+//                kInitScan entries (one free hook per vertex).
 //  * cc_hook   - one pass over the vertices, 32 per warp.  Lists of <= 16
 //                entries are walked by their own lane; lists of up to
 //                kChunk entries are walked by the whole warp (ballot loop,
@@ -32,6 +33,7 @@ using namespace dev;
 constexpr int kTPB = 256;
 constexpr int kLaneMax = 16;   // lists up to this length: lane-level
 constexpr int kChunk = 2048;   // lists longer than this: chunk records
+constexpr int kInitScan = 8;   // entries cc_init looks at for a first smaller neighbour
 
 // Row [beg, end) of v, or empty when the row is malformed (cc_init reports it).
 __device__ __forceinline__ void cc_row(const int* nindex, int v, int m, int& beg, int& end) {
@@ -95,8 +97,12 @@ __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restr
       raise(status, ECL_ERR_BAD_GRAPH, v);
       beg = end = 0;
     }
+    // Only the first few entries are looked at: the hook is an optional head
+    // start (the labels do not depend on it), and scanning a whole hub row
+    // from one thread would serialise a 163k-entry R-MAT hub.
     int p = v;
-    for (int i = beg; i < end; i++) {
+    const int stop = min(end, beg + kInitScan);
+    for (int i = beg; i < stop; i++) {
       const int u = __ldg(&nlist[i]);
       if (u < v && u >= 0) {
         p = u;

@@ -1,27 +1,37 @@
 // Graph colouring (ECL-GC contract).
 //
-// Result contract (src/racefree/egr-input/GC/ECL-GC-atomic.cu): a vertex's
-// colour is chosen among [0, r] where r is its number of higher-priority list
-// entries, priority being (degree, hash, id) (:102).  init/runLarge/runSmall
-// (:78-303) only fix a colour once it is the smallest colour not taken by a
-// decided higher-priority neighbour and no undecided higher-priority
-// neighbour can still take it, which yields the first-fit greedy colouring in
-// descending priority order -- a schedule-independent result.
+// Result contract (src/racefree/egr-input/GC/ECL-GC-atomic.cu): priorities
+// are (degree, hash, id) (:102); init/runLarge/runSmall (:78-303) only fix a
+// colour once it is the smallest colour not taken by a decided higher-priority
+// list entry and no undecided one can still take it, i.e. the result is the
+// first-fit greedy colouring in descending priority order.  Self-loops are
+// never higher priority (:102 compares v with itself) and are ignored.
 //
-// B200 design (Jones-Plassmann with window shortcutting):
-//  * gc_init compacts each vertex's higher-priority entries into hl[] at the
-//    vertex's own CSR offset (lane-serial for short lists, warp ballot +
-//    popc compaction for long ones) and sets state[v] = (lo=0, hi=r).
-//  * state[v] is one 32-bit word (lo << 16 | hi): lo = smallest colour v can
-//    still get, hi = r, an upper bound.  lo == hi means decided (colour lo).
-//    r <= sqrt(edges) < 46341, so 16 bits each suffice.
-//  * gc_run is ONE persistent launch.  Each undecided vertex scans its hl
-//    list once per sweep, building two 64-bit masks over the colour window
-//    [lo, lo+64): colours of decided neighbours, and the union of the
-//    possible-colour windows of undecided neighbours.  The first free colour
-//    c in the window is v's colour as soon as no undecided neighbour can
-//    take it; otherwise lo advances to c.  Long lists are scanned by the
-//    whole warp with the masks OR-reduced by __reduce_or_sync.
+// B200 design: greedy colouring pulled in priority order.
+//  * gc_init / gc_init_chunks (degree-binned: lane / warp / 256-entry chunk
+//    records) compact every row's higher-priority entries to the front of
+//    the row's slot in nl2[]; hc[v] = their number.
+//  * gc_keys + radix_sort_pairs rank all vertices by priority (a stable LSD
+//    sort on the inverted (degree, hash) key over ids in descending order),
+//    which is a topological order of the colouring dependencies.
+//  * gc_pull is ONE cooperative persistent launch.  Warps claim ranks in that
+//    order -- one long row (> 32 entries; they form a prefix of the order,
+//    priority being degree-first) or 32 short rows at a time; each vertex
+//    waits (bounded polling of exactly its
+//    own higher-priority neighbours' colour words -- no shared hot spot) until
+//    they are coloured and stores the smallest colour they do not use.
+//    Because claims follow the topological order, the lowest unfinished rank
+//    always has all its dependencies finished, so the launch always makes
+//    progress.  There is no push, no counter and no queue: the total work is
+//    one read of every higher-priority entry, and the longest priority chain
+//    (about 2700 vertices at R-MAT-22, most of it in the hub core) costs one
+//    poll-and-store hop per vertex on it.
+//  * A long row is scanned by a whole warp with a 2048-colour bitmap in
+//    shared memory; claiming one long row per warp keeps every in-flight row
+//    of the dense hub core scanning concurrently, so a hop along the chain
+//    costs one poll, not a scan of the row.
+#include "csr_bins.cuh"
+#include "radix_sort.cuh"
 #include "runtime.cuh"
 
 namespace ecl {
@@ -30,7 +40,18 @@ namespace {
 using namespace dev;
 
 constexpr int kTPB = 256;
-constexpr int kLaneMax = 32;
+
+constexpr int kWarpRow = 32;  // rows longer than this are coloured by a whole warp
+
+struct GCCtl {
+  int head_big;    // next rank to claim among the long rows, [0, nbig)
+  int pad0[31];
+  int head_small;  // next rank to claim among the short rows, [nbig, n)
+  int pad1[31];
+  int nchunks;
+  int nbig;        // rows longer than kWarpRow: a prefix of the priority order
+  int pad2[30];
+};
 
 __device__ __forceinline__ bool gc_outranks(int du, unsigned hu, int u, int dv, unsigned hv, int v) {
   if (du != dv) return du > dv;
@@ -38,188 +59,253 @@ __device__ __forceinline__ bool gc_outranks(int du, unsigned hu, int u, int dv, 
   return u > v;
 }
 
+// 0: ignore (self-loop or invalid), 1: higher priority, 2: lower priority.
+__device__ __forceinline__ int gc_class(int u, int v, int dv, unsigned hv, int n, const int* nindex, Status* status) {
+  if ((unsigned)u >= (unsigned)n) {
+    raise(status, ECL_ERR_BAD_GRAPH, u);
+    return 0;
+  }
+  if (u == v) return 0;
+  const int du = __ldg(&nindex[u + 1]) - __ldg(&nindex[u]);
+  return gc_outranks(du, ecl_hash((unsigned)u), u, dv, hv, v) ? 1 : 2;
+}
+
 __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restrict__ nindex,
-                                                const int* __restrict__ nlist, int* __restrict__ hl,
-                                                int* __restrict__ hc, unsigned* __restrict__ state,
-                                                int* __restrict__ color, Status* __restrict__ status) {
+                                                const int* __restrict__ nlist, int* __restrict__ nl2,
+                                                int* __restrict__ hc, RowChunks rc,
+                                                Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   for (int base = warp * 32; base < n; base += nwarps * 32) {
     const int v = base + lane;
     int beg = 0, end = 0;
-    if (v < n) {
-      beg = __ldg(&nindex[v]);
-      end = __ldg(&nindex[v + 1]);
-      if (beg < 0 || end < beg || end > m) {
-        raise(status, ECL_ERR_BAD_GRAPH, v);
-        beg = end = 0;
-      }
-    }
+    if (v < n) csr_row(nindex, v, m, beg, end, status);
     const int dv = end - beg;
     const unsigned hv = ecl_hash((unsigned)v);
-    int cnt = 0;
-    const bool big = dv > kLaneMax;
-    if (v < n && !big) {
+    int h = 0;
+    if (dv > kBinChunk) push_row_chunks(rc, v, beg, end);
+    if (v < n && dv <= kBinLane) {
       for (int i = beg; i < end; i++) {
         const int u = __ldg(&nlist[i]);
-        if ((unsigned)u >= (unsigned)n) {
-          raise(status, ECL_ERR_BAD_GRAPH, u);
-          continue;
-        }
-        const int du = __ldg(&nindex[u + 1]) - __ldg(&nindex[u]);
-        if (gc_outranks(du, ecl_hash((unsigned)u), u, dv, hv, v)) hl[beg + cnt++] = u;
+        const int k = gc_class(u, v, dv, hv, n, nindex, status);
+        if (k == 1) nl2[beg + h++] = u;
       }
     }
-    unsigned todo = __ballot_sync(kFull, big);
+    unsigned todo = __ballot_sync(kFull, dv > kBinLane && dv <= kBinChunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
       const int wv = __shfl_sync(kFull, v, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      const int wdv = wend - wbeg;
       const unsigned whv = ecl_hash((unsigned)wv);
-      int wcnt = 0;
+      int wh = 0;
       for (int i0 = wbeg; i0 < wend; i0 += 32) {
-        const int i = i0 + lane;
-        bool keep = false;
-        int u = 0;
-        if (i < wend) {
-          u = __ldg(&nlist[i]);
-          if ((unsigned)u < (unsigned)n) {
-            const int du = __ldg(&nindex[u + 1]) - __ldg(&nindex[u]);
-            keep = gc_outranks(du, ecl_hash((unsigned)u), u, wdv, whv, wv);
-          } else {
-            raise(status, ECL_ERR_BAD_GRAPH, u);
-          }
+        int k = 0, u = 0;
+        if (i0 + lane < wend) {
+          u = __ldg(&nlist[i0 + lane]);
+          k = gc_class(u, wv, wend - wbeg, whv, n, nindex, status);
         }
-        const unsigned bal = __ballot_sync(kFull, keep);
-        if (keep) hl[wbeg + wcnt + __popc(bal & ((1u << lane) - 1))] = u;
-        wcnt += __popc(bal);
+        const unsigned bh = __ballot_sync(kFull, k == 1);
+        if (k == 1) nl2[wbeg + wh + __popc(bh & ((1u << lane) - 1))] = u;
+        wh += __popc(bh);
       }
-      if (lane == who) cnt = wcnt;
+      if (lane == who) h = wh;
     }
-    if (v < n) {
-      if (cnt > 0xffff) raise(status, ECL_ERR_UNSUPPORTED, v);
-      hc[v] = cnt;
-      state[v] = (unsigned)cnt & 0xffffu;  // lo = 0, hi = cnt; cnt == 0 means decided colour 0
-      if (cnt == 0) color[v] = 0;
-    }
+    if (v < n) hc[v] = dv > kBinChunk ? 0 : h;  // chunked rows start at 0, counted by gc_init_chunks
   }
 }
 
-// Folds neighbour state s into the masks of window [lo, lo+64).
-__device__ __forceinline__ void gc_fold(unsigned s, int lo, unsigned long long& used, unsigned long long& cover) {
-  const int slo = (int)(s >> 16), shi = (int)(s & 0xffffu);
-  if (slo == shi) {
-    const int d = slo - lo;
-    if (d >= 0 && d < 64) used |= 1ull << d;
-  } else {
-    const int a = max(slo, lo) - lo, b = min(shi, lo + 63) - lo;
-    if (a <= b) {
-      const unsigned long long hiMask = (b >= 63) ? ~0ull : ((1ull << (b + 1)) - 1);
-      cover |= hiMask & ~((1ull << a) - 1);
-    }
-  }
-}
-
-// Applies one scan's result to v.  Returns true when v is still undecided.
-__device__ __forceinline__ bool gc_apply(int v, int lo, int hi, unsigned long long used, unsigned long long cover,
-                                         unsigned* state, int* color) {
-  if (used == ~0ull) {  // the whole window is taken by decided neighbours
-    const int nlo = lo + 64;  // <= hi: 64 + lo decided neighbours exist
-    if (nlo >= hi) {
-      color[v] = hi;
-      st(&state[v], ((unsigned)hi << 16) | (unsigned)hi);
-      return false;
-    }
-    st(&state[v], ((unsigned)nlo << 16) | (unsigned)hi);
-    return true;
-  }
-  const int c = __ffsll((long long)~used) - 1;
-  const int col = lo + c;
-  if (((cover >> c) & 1ull) == 0 || col == hi) {
-    color[v] = col;
-    st(&state[v], ((unsigned)col << 16) | (unsigned)col);
-    return false;
-  }
-  if (col != lo) st(&state[v], ((unsigned)col << 16) | (unsigned)hi);
-  return true;
-}
-
-__global__ void __launch_bounds__(kTPB) gc_run(int n, const int* __restrict__ nindex, const int* __restrict__ hl,
-                                               const int* __restrict__ hc, unsigned* __restrict__ state,
-                                               int* __restrict__ color, Status* __restrict__ status,
-                                               int max_sweeps) {
+__global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restrict__ nindex,
+                                                       const int* __restrict__ nlist, int* __restrict__ nl2,
+                                                       int* __restrict__ hc, RowChunks rc,
+                                                       Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  int sweep = 0;
-  for (;; sweep++) {
-    bool missing = false;
-    for (int base = warp * 32; base < n; base += nwarps * 32) {
-      const int v = base + lane;
-      unsigned s = 0;
-      if (v < n) s = ld(&state[v]);
-      const int lo = (int)(s >> 16), hi = (int)(s & 0xffffu);
-      const bool und = (v < n) && lo != hi;
-      if (!__any_sync(kFull, und)) continue;
-      int beg = 0, cnt = 0;
-      if (und) {
-        beg = __ldg(&nindex[v]);
-        cnt = __ldg(&hc[v]);
+  const int total = *rc.count;
+  for (int c = warp; c < total; c += nwarps) {
+    const int2 r = rc.rec[c];
+    const int v = r.x;
+    const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
+    const int stop = min(r.y + kBinChunk, end);
+    const unsigned hv = ecl_hash((unsigned)v);
+    for (int i0 = r.y; i0 < stop; i0 += 32) {
+      int k = 0, u = 0;
+      if (i0 + lane < stop) {
+        u = __ldg(&nlist[i0 + lane]);
+        k = gc_class(u, v, end - beg, hv, n, nindex, status);
       }
-      const bool big = und && cnt > kLaneMax;
-      if (und && !big) {
-        unsigned long long used = 0, cover = 0;
-        for (int i = beg; i < beg + cnt; i++) gc_fold(ld(&state[__ldg(&hl[i])]), lo, used, cover);
-        missing |= gc_apply(v, lo, hi, used, cover, state, color);
-      }
-      unsigned todo = __ballot_sync(kFull, big);
-      while (todo) {
-        const int who = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const int wv = __shfl_sync(kFull, v, who);
-        const int wbeg = __shfl_sync(kFull, beg, who);
-        const int wend = wbeg + __shfl_sync(kFull, cnt, who);
-        const int wlo = __shfl_sync(kFull, lo, who);
-        const int whi = __shfl_sync(kFull, hi, who);
-        unsigned long long used = 0, cover = 0;
-        for (int i = wbeg + lane; i < wend; i += 32) gc_fold(ld(&state[__ldg(&hl[i])]), wlo, used, cover);
-        const unsigned ul = __reduce_or_sync(kFull, (unsigned)used);
-        const unsigned uh = __reduce_or_sync(kFull, (unsigned)(used >> 32));
-        const unsigned cl = __reduce_or_sync(kFull, (unsigned)cover);
-        const unsigned ch = __reduce_or_sync(kFull, (unsigned)(cover >> 32));
-        if (lane == who) {
-          used = ((unsigned long long)uh << 32) | ul;
-          cover = ((unsigned long long)ch << 32) | cl;
-          missing |= gc_apply(wv, wlo, whi, used, cover, state, color);
-        }
-      }
-    }
-    if (!__any_sync(kFull, missing)) break;
-    if (sweep >= max_sweeps) {
-      if (lane == 0) raise(status, ECL_ERR_NO_CONVERGENCE, warp);
-      break;
+      const unsigned bh = __ballot_sync(kFull, k == 1);
+      int hbase = 0;
+      if (lane == 0 && bh) hbase = fetch_add(&hc[v], __popc(bh));
+      hbase = __shfl_sync(kFull, hbase, 0);
+      if (k == 1) nl2[beg + hbase + __popc(bh & ((1u << lane) - 1))] = u;
     }
   }
-  if (lane == 0) fetch_max(&status->rounds, sweep + 1);
 }
 
-void gc_layout(Carve& c, int n, int m, int** hl, int** hc, unsigned** state) {
-  *hl = c.take<int>((size_t)(m > 0 ? m : 1));
-  *hc = c.take<int>((size_t)n);
-  *state = c.take<unsigned>((size_t)n);
+// Sort keys: ascending order of ~((degree << 32) | hash) is descending
+// (degree, hash); the values start in descending id order, so the stable
+// sort breaks the remaining ties by descending id -- exactly the priority.
+__global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ nindex,
+                                                unsigned long long* __restrict__ keys, int* __restrict__ vals,
+                                                GCCtl* __restrict__ ctl) {
+  for (int base = (blockIdx.x * kTPB + threadIdx.x) & ~31; base < n; base += gridDim.x * kTPB) {
+    const int i = base + (threadIdx.x & 31);
+    bool big = false;
+    if (i < n) {
+      const int v = n - 1 - i;
+      const unsigned deg = (unsigned)(__ldg(&nindex[v + 1]) - __ldg(&nindex[v]));
+      keys[i] = ~(((unsigned long long)deg << 32) | ecl_hash((unsigned)v));
+      vals[i] = v;
+      big = deg > (unsigned)kWarpRow;
+    }
+    const int nb = __popc(__ballot_sync(kFull, big));
+    if ((threadIdx.x & 31) == 0 && nb) fetch_add(&ctl->nbig, nb);
+  }
+}
+
+__device__ __forceinline__ unsigned long long gc_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+constexpr unsigned long long kStallNs = 2000000000ull;  // 2 s without progress -> give up
+constexpr int kMexWords = 64;                           // warp bitmap: 2048 colours per pass
+
+// Colour of u once it is published (bounded wait).  Returns -1 on a stall.
+__device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* status) {
+  int c = ld(&color[u]);
+  if (c >= 0) return c;
+  unsigned nap = 32, spins = 0;
+  const unsigned long long t0 = gc_now();
+  while ((c = ld(&color[u])) < 0) {
+    if (++spins > (1u << 24) || gc_now() - t0 > kStallNs || ld(&status->code) != 0) {
+      raise(status, ECL_ERR_NO_CONVERGENCE, u);
+      return -1;
+    }
+    __nanosleep(nap);
+    nap = min(nap * 2, 512u);
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
+                                                const int* __restrict__ hc, const int* __restrict__ order,
+                                                int* __restrict__ color, GCCtl* __restrict__ ctl,
+                                                Status* __restrict__ status) {
+  __shared__ unsigned s_bits[kTPB / 32][kMexWords];
+  const int lane = threadIdx.x & 31;
+  unsigned* bits = s_bits[threadIdx.x >> 5];
+  const int nbig = ld(&ctl->nbig);
+  // Long rows, ONE per warp claim: every long row in flight scans its
+  // higher-priority list concurrently, so when its last dependency is
+  // coloured only that entry remains (a warp holding several would scan
+  // them one after another, on the critical path of the dense hub core).
+  while (true) {
+    int r = 0;
+    if (lane == 0) r = fetch_add(&ctl->head_big, 1);
+    r = __shfl_sync(kFull, r, 0);
+    if (r >= nbig) break;
+    const int wv = __ldg(&order[r]);
+    const int wb = __ldg(&nindex[wv]);
+    const int we = wb + __ldg(&hc[wv]);
+    int off = 0, c = -1;
+    while (c < 0) {
+      bits[lane] = 0;
+      bits[lane + 32] = 0;
+      __syncwarp();
+      bool stalled = false;
+      for (int i = wb + lane; i < we; i += 32) {
+        const int cu = gc_wait_colour(color, __ldg(&nl2[i]), status);
+        if (cu < 0) {
+          stalled = true;
+          break;
+        }
+        const int d = cu - off;
+        if (d >= 0 && d < 32 * kMexWords) atomicOr(&bits[d >> 5], 1u << (d & 31));
+      }
+      if (__any_sync(kFull, stalled)) return;
+      __syncwarp();
+      const unsigned w0 = bits[lane], w1 = bits[lane + 32];
+      const unsigned f0 = __ballot_sync(kFull, w0 != ~0u), f1 = __ballot_sync(kFull, w1 != ~0u);
+      if (f0) {
+        const int wi = __ffs(f0) - 1;
+        c = off + wi * 32 + __ffs(~__shfl_sync(kFull, w0, wi)) - 1;
+      } else if (f1) {
+        const int wi = __ffs(f1) - 1;
+        c = off + (wi + 32) * 32 + __ffs(~__shfl_sync(kFull, w1, wi)) - 1;
+      }
+      __syncwarp();
+      off += 32 * kMexWords;
+    }
+    if (lane == 0) st(&color[wv], c);
+    __syncwarp();
+  }
+  // Short rows: 32 ranks per claim, every lane its own vertex.
+  while (true) {
+    int base = 0;
+    if (lane == 0) base = nbig + fetch_add(&ctl->head_small, 32);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= n) return;
+    const int r = base + lane;
+    int v = -1, beg = 0, h = 0;
+    if (r < n) {
+      v = __ldg(&order[r]);
+      beg = __ldg(&nindex[v]);
+      h = __ldg(&hc[v]);
+    }
+    // colour <= h <= 32: one 64-bit mask
+    if (v >= 0) {
+      unsigned long long used = 0;
+      bool ok = true;
+      for (int i = beg; i < beg + h; i++) {
+        const int cu = gc_wait_colour(color, __ldg(&nl2[i]), status);
+        if (cu < 0) {
+          ok = false;
+          break;
+        }
+        if (cu < 64) used |= 1ull << cu;
+      }
+      if (ok) st(&color[v], __ffsll((long long)~used) - 1);
+    }
+    if (__any_sync(kFull, ld(&status->code) != 0)) return;
+  }
+}
+
+struct GCBufs {
+  GCCtl* ctl;
+  int* nl2;
+  int* hc;
+  unsigned long long* keys0;
+  unsigned long long* keys1;
+  int* vals0;
+  int* vals1;
+  unsigned* sort_temp;
+  int2* chunks;
+};
+
+void gc_layout(Carve& c, int n, int m, GCBufs* b) {
+  b->ctl = c.take<GCCtl>(1);
+  b->nl2 = c.take<int>((size_t)(m > 0 ? m : 1));
+  b->hc = c.take<int>((size_t)n);
+  b->keys0 = c.take<unsigned long long>((size_t)n);
+  b->keys1 = c.take<unsigned long long>((size_t)n);
+  b->vals0 = c.take<int>((size_t)n);
+  b->vals1 = c.take<int>((size_t)n);
+  b->sort_temp = c.take<unsigned>(radix_temp_words((size_t)n));
+  b->chunks = c.take<int2>(row_chunk_capacity(m));
 }
 
 }  // namespace
 
 size_t gc_workspace_bytes(int n, int m) {
   Carve c;
-  int *hl, *hc;
-  unsigned* state;
-  gc_layout(c, n, m, &hl, &hc, &state);
+  GCBufs b;
+  gc_layout(c, n, m, &b);
   return c.bytes();
 }
 
@@ -239,19 +325,34 @@ extern "C" ecl_status ecl_gc(const ecl_graph_view* g, int32_t* color_out, ecl_op
   int* color = s.output(color_out, (size_t)s.n);
   if (!color) return s.finish(ECL_ERR_OOM);
   Carve c{s.ws};
-  int *hl, *hc;
-  unsigned* state;
-  gc_layout(c, s.n, s.m, &hl, &hc, &state);
+  GCBufs b;
+  gc_layout(c, s.n, s.m, &b);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
+    return s.finish(ECL_ERR_CUDA);
+  const int coop_grid = s.dev.sms * occ;
   const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-  // Warps sweep asynchronously, so one warp may sweep many times while it
-  // waits on a vertex owned by a slower warp: the cap is a fixed backstop
-  // (GC cannot stall -- priorities form a DAG), not a per-graph bound.
-  const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : (1 << 22);
+  const RowChunks rc{b.chunks, &b.ctl->nchunks};
+  // key bits that vary: 32 hash bits + enough bits for any degree <= m
+  int degbits = 1;
+  while (degbits < 31 && ((long long)1 << degbits) <= (long long)s.m) degbits++;
 
   s.start_timer();
-  ECL_LAUNCH(gc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, hl, hc, state, color, s.status);
+  if (cudaMemsetAsync(b.ctl, 0, sizeof(GCCtl), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
+  if (cudaMemsetAsync(color, 0xff, sizeof(int) * (size_t)s.n, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
+  ECL_LAUNCH(gc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.nl2, b.hc, rc, s.status);
+  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.nl2, b.hc, rc, s.status);
   s.mark();
-  ECL_LAUNCH(gc_run, grid, kTPB, 0, s.stream, s.n, s.nindex, hl, hc, state, color, s.status, max_sweeps);
+  ECL_LAUNCH(gc_keys, grid, kTPB, 0, s.stream, s.n, s.nindex, b.keys0, b.vals0, b.ctl);
+  const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, s.n, 0, 32 + degbits, b.sort_temp, s.stream);
+  const int* order = in1 ? b.vals1 : b.vals0;
+  s.mark();
+  int n_ = s.n;
+  const int* nindex_ = s.nindex;
+  void* args[] = {&n_, &nindex_, &b.nl2, &b.hc, &order, &color, &b.ctl, &s.status};
+  if (cudaLaunchCooperativeKernel((void*)gc_pull, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
+    return s.finish(ECL_ERR_CUDA);
+  count_launch();
   s.mark();
   s.stop_timer();
   return s.finish();

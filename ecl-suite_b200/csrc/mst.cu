@@ -35,7 +35,7 @@ typedef unsigned long long u64;
 
 constexpr int kTPB = 256;
 constexpr int kLaneMax = 32;
-constexpr int kChunk = 4096;
+constexpr int kChunk = 256;  // R-MAT's heavy low-id rows share warp groups: keep warp-level rows short
 constexpr int kMaxRounds = 64;
 constexpr int kSamples = 1024;
 

@@ -13,7 +13,8 @@
 //  * scc_mark / scc_build trim first: a vertex with no in-entry or no
 //    out-entry (self-loops ignored) is its own SCC and contributes no edge;
 //    only edges between two untrimmed vertices enter the int2 worklist
-//    (warp-aggregated appends);
+//    (warp-aggregated appends).  Both passes are degree-binned (lane / warp /
+//    256-entry chunk records), so hub rows spread over all warps;
 //  * scc_solve runs EVERY propagation sweep and every trimming round in one
 //    cooperative persistent launch, separated by bounded grid barriers (the
 //    reference pays a host round trip per propagation launch, :283-287);
@@ -21,6 +22,7 @@
 //    sweep jumps through imax[imax[v]] / omax[omax[w]] (both still valid
 //    bounds) so values travel many hops per sweep;
 //  * the final labels are written by the same launch (label = in-max).
+#include "csr_bins.cuh"
 #include "grid_sync.cuh"
 #include "runtime.cuh"
 
@@ -45,10 +47,25 @@ struct SCCRound {
   int again;
 };
 
+// A vertex is live (can be in a non-trivial SCC) iff it has an in-entry and an
+// out-entry other than self-loops.  scc_mark sets hasin[w] for every entry
+// w != v (plain relaxed stores of 1: idempotent) and hasout[v] for every v
+// with such an entry; rows longer than kBinChunk go to chunk records.
+__device__ __forceinline__ void scc_mark_entry(bool valid, int v, int w, int n, int* hasin, bool& out,
+                                               Status* status) {
+  if (!valid) return;
+  if ((unsigned)w >= (unsigned)n) {
+    raise(status, ECL_ERR_BAD_GRAPH, w);
+  } else if (w != v) {
+    st(&hasin[w], 1);
+    out = true;
+  }
+}
+
 __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __restrict__ nindex,
                                                  const int* __restrict__ nlist, int* __restrict__ hasin,
-                                                 int* __restrict__ imax, int* __restrict__ omax,
-                                                 Status* __restrict__ status) {
+                                                 int* __restrict__ hasout, int* __restrict__ imax,
+                                                 int* __restrict__ omax, RowChunks rc, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -56,86 +73,84 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     const int v = base + lane;
     int beg = 0, end = 0;
     if (v < n) {
-      beg = __ldg(&nindex[v]);
-      end = __ldg(&nindex[v + 1]);
-      if (beg < 0 || end < beg || end > m) {
-        raise(status, ECL_ERR_BAD_GRAPH, v);
-        beg = end = 0;
-      }
+      csr_row(nindex, v, m, beg, end, status);
       imax[v] = v;
       omax[v] = v;
     }
-    const int kmax = __reduce_max_sync(kFull, (end - beg) <= 32 ? end - beg : 0);
+    const int deg = end - beg;
+    if (deg > kBinChunk) push_row_chunks(rc, v, beg, end);
+    bool out = false;
+    const bool lanelvl = deg <= kBinLane;
+    const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k = 0; k < kmax; k++) {
-      if (k < end - beg && end - beg <= 32) {
-        const int w = __ldg(&nlist[beg + k]);
-        if ((unsigned)w >= (unsigned)n) raise(status, ECL_ERR_BAD_GRAPH, w);
-        else if (w != v) st(&hasin[w], 1);
-      }
+      const bool valid = lanelvl && k < deg;
+      scc_mark_entry(valid, v, valid ? __ldg(&nlist[beg + k]) : 0, n, hasin, out, status);
     }
-    unsigned todo = __ballot_sync(kFull, end - beg > 32);
+    unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
       const int wv = __shfl_sync(kFull, v, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      for (int i = wbeg + lane; i < wend; i += 32) {
-        const int w = __ldg(&nlist[i]);
-        if ((unsigned)w >= (unsigned)n) raise(status, ECL_ERR_BAD_GRAPH, w);
-        else if (w != wv) st(&hasin[w], 1);
-      }
+      bool wout = false;
+      for (int i = wbeg + lane; i < wend; i += 32) scc_mark_entry(true, wv, __ldg(&nlist[i]), n, hasin, wout, status);
+      if (__any_sync(kFull, wout) && lane == who) out = true;
     }
+    if (v < n) hasout[v] = (deg <= kBinChunk && out) ? 1 : 0;  // long rows: set by scc_mark_chunks
   }
 }
 
-// True when v has an out-entry other than a self-loop.
-__device__ __forceinline__ bool scc_has_out(const int* nindex, const int* nlist, int v, int m) {
-  const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
-  if (beg < 0 || end < beg || end > m) return false;
-  for (int i = beg; i < end; i++)
-    if (__ldg(&nlist[i]) != v) return true;
-  return false;
+__global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
+                                                        const int* __restrict__ nlist, int* __restrict__ hasin,
+                                                        int* __restrict__ hasout, RowChunks rc,
+                                                        Status* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  const int total = *rc.count;
+  for (int c = warp; c < total; c += nwarps) {
+    const int2 r = rc.rec[c];
+    const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
+    bool out = false;
+    for (int i = r.y + lane; i < end; i += 32) scc_mark_entry(true, r.x, __ldg(&nlist[i]), n, hasin, out, status);
+    if (__any_sync(kFull, out) && lane == 0) st(&hasout[r.x], 1);
+  }
 }
 
-__device__ __forceinline__ int scc_slot(int* counter, bool pred, int lane) {
-  const unsigned bal = __ballot_sync(kFull, pred);
-  if (bal == 0) return -1;
-  int base = 0;
-  if (lane == 0) base = fetch_add(counter, __popc(bal));
-  base = __shfl_sync(kFull, base, 0);
-  return pred ? base + __popc(bal & ((1u << lane) - 1)) : -1;
+__device__ __forceinline__ bool scc_live(const int* hasin, const int* hasout, int v) {
+  return ld(&hasin[v]) != 0 && ld(&hasout[v]) != 0;
 }
 
 __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __restrict__ nindex,
                                                   const int* __restrict__ nlist, const int* __restrict__ hasin,
-                                                  int2* __restrict__ wl, SCCCtl* __restrict__ ctl) {
+                                                  const int* __restrict__ hasout, int2* __restrict__ wl,
+                                                  SCCCtl* __restrict__ ctl) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   for (int base = warp * 32; base < n; base += nwarps * 32) {
     const int v = base + lane;
     int beg = 0, end = 0;
-    bool live = false;
-    if (v < n && ld(&hasin[v])) {
+    if (v < n && scc_live(hasin, hasout, v)) {
       beg = __ldg(&nindex[v]);
       end = __ldg(&nindex[v + 1]);
       if (beg < 0 || end < beg || end > m) beg = end = 0;
-      live = end > beg;
     }
-    const bool lanelvl = live && end - beg <= 32;
-    const int kmax = __reduce_max_sync(kFull, lanelvl ? end - beg : 0);
+    const int deg = end - beg;
+    const bool lanelvl = deg <= kBinLane;
+    const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k = 0; k < kmax; k++) {
       bool keep = false;
       int w = 0;
-      if (lanelvl && k < end - beg) {
+      if (lanelvl && k < deg) {
         w = __ldg(&nlist[beg + k]);
-        keep = w != v && (unsigned)w < (unsigned)n && ld(&hasin[w]) && scc_has_out(nindex, nlist, w, m);
+        keep = w != v && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
       }
-      const int at = scc_slot(&ctl->nedges, keep, lane);
+      const int at = warp_append(&ctl->nedges, keep);
       if (keep) wl[at] = make_int2(v, w);
     }
-    unsigned todo = __ballot_sync(kFull, live && end - beg > 32);
+    unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
@@ -147,11 +162,36 @@ __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __res
         int w = 0;
         if (i0 + lane < wend) {
           w = __ldg(&nlist[i0 + lane]);
-          keep = w != wv && (unsigned)w < (unsigned)n && ld(&hasin[w]) && scc_has_out(nindex, nlist, w, m);
+          keep = w != wv && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
         }
-        const int at = scc_slot(&ctl->nedges, keep, lane);
+        const int at = warp_append(&ctl->nedges, keep);
         if (keep) wl[at] = make_int2(wv, w);
       }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTPB) scc_build_chunks(int n, const int* __restrict__ nindex,
+                                                         const int* __restrict__ nlist, const int* __restrict__ hasin,
+                                                         const int* __restrict__ hasout, int2* __restrict__ wl,
+                                                         SCCCtl* __restrict__ ctl, RowChunks rc) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  const int total = *rc.count;
+  for (int c = warp; c < total; c += nwarps) {
+    const int2 r = rc.rec[c];
+    if (!scc_live(hasin, hasout, r.x)) continue;  // warp-uniform
+    const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
+    for (int i0 = r.y; i0 < end; i0 += 32) {
+      bool keep = false;
+      int w = 0;
+      if (i0 + lane < end) {
+        w = __ldg(&nlist[i0 + lane]);
+        keep = w != r.x && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
+      }
+      const int at = warp_append(&ctl->nedges, keep);
+      if (keep) wl[at] = make_int2(r.x, w);
     }
   }
 }
@@ -213,7 +253,7 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA,
         const int iv = ld(&imax[e.x]), ov = ld(&omax[e.x]);
         keep = iv != ov && iv == ld(&imax[e.y]) && ov == ld(&omax[e.y]);
       }
-      const int at = scc_slot(&rounds[round].size, keep, lane);
+      const int at = warp_append(&rounds[round].size, keep);
       if (keep) nxt[at] = e;
     }
     if (!grid_sync(&ctl->bar, status)) return;
@@ -244,6 +284,9 @@ struct SCCBufs {
   SCCCtl* ctl;
   SCCRound* rounds;
   int* hasin;
+  int* hasout;
+  int* nchunks;
+  int2* chunks;
   int* imax;
   int* omax;
   int2* wlA;
@@ -256,6 +299,9 @@ void scc_layout(Carve& c, int n, int m, SCCBufs* b) {
   b->max_rounds = n + 1;
   b->rounds = c.take<SCCRound>((size_t)b->max_rounds);
   b->hasin = c.take<int>((size_t)n);
+  b->hasout = c.take<int>((size_t)n);
+  b->nchunks = c.take<int>(64);
+  b->chunks = c.take<int2>(row_chunk_capacity(m));
   b->imax = c.take<int>((size_t)n);
   b->omax = c.take<int>((size_t)n);
   b->wlA = c.take<int2>((size_t)(m > 0 ? m : 1));
@@ -299,9 +345,14 @@ extern "C" ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label_out, ecl_o
   if (cudaMemsetAsync(b.rounds, 0, sizeof(SCCRound) * (size_t)b.max_rounds, s.stream) != cudaSuccess)
     return s.finish(ECL_ERR_CUDA);
   if (cudaMemsetAsync(b.hasin, 0, sizeof(int) * (size_t)s.n, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.imax, b.omax, s.status);
+  if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
+  const RowChunks rc{b.chunks, b.nchunks};
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.hasout, b.imax, b.omax, rc,
+             s.status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.hasin, b.hasout, rc, s.status);
   s.mark();
-  ECL_LAUNCH(scc_build, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.wlA, b.ctl);
+  ECL_LAUNCH(scc_build, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.hasout, b.wlA, b.ctl);
+  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.hasin, b.hasout, b.wlA, b.ctl, rc);
   s.mark();
   int n_ = s.n;
   void* args[] = {&n_, &b.wlA, &b.wlB, &b.imax, &b.omax, &label, &b.ctl, &b.rounds, &max_rounds, &s.status};
