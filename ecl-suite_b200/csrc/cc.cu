@@ -21,7 +21,7 @@
 //  * cc_flatten- label[v] = root(v).
 // The parent array IS the output label array (no extra n-sized buffer).
 // All parent accesses are device-scope relaxed atomics; links use CAS.
-#include "runtime.cuh"
+#include "solvers.cuh"
 
 #include <mutex>
 
@@ -213,6 +213,29 @@ size_t cc_workspace_bytes(int n, int m) {
 
 }  // namespace ecl
 
+namespace ecl {
+
+ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, const DeviceInfo& dev,
+                      cudaStream_t stream, Marker mark) {
+  Carve c{ws};
+  CCCounters* ctr;
+  int2* chunks;
+  cc_layout(c, g.n, g.m, &ctr, &chunks);
+  const int grid = dev.grid_blocks(kTPB);
+  ECL_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(CCCounters), stream));
+  ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
+  mark();
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, ctr, status);
+  mark();
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, chunks, ctr, status);
+  mark();
+  ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
+  mark();
+  return ECL_OK;
+}
+
+}  // namespace ecl
+
 extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* opts) {
   using namespace ecl;
   ecl_opts local{};
@@ -223,24 +246,16 @@ extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* 
   if (st != ECL_OK) return s.finish(st);
   int* parent = s.output(label, (size_t)s.n);
   if (!parent) return s.finish(ECL_ERR_OOM);
-  Carve c{s.ws};
-  CCCounters* ctr;
-  int2* chunks;
-  cc_layout(c, s.n, s.m, &ctr, &chunks);
-  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-
+  GraphDev gd;
+  gd.n = s.n;
+  gd.m = s.m;
+  gd.nindex = s.nindex;
+  gd.nlist = s.nlist;
+  gd.flags = g->flags;
   s.start_timer();
-  if (cudaMemsetAsync(ctr, 0, sizeof(CCCounters), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  ECL_LAUNCH(cc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, s.status);
-  s.mark();
-  ECL_LAUNCH(cc_hook, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, parent, chunks, ctr, s.status);
-  s.mark();
-  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, parent, chunks, ctr, s.status);
-  s.mark();
-  ECL_LAUNCH(cc_flatten, grid, kTPB, 0, s.stream, s.n, parent);
-  s.mark();
+  st = cc_enqueue(gd, parent, s.ws, s.status, s.dev, s.stream, Marker{&s});
   s.stop_timer();
-  return s.finish();
+  return s.finish(st);
 }
 
 // ---- allocation-free variant --------------------------------------------------
@@ -308,7 +323,7 @@ extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t
   // The array keeps the previous call's contents: clear the status block and
   // the counters (adjacent, at the front of the array) before every solve.
   ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
-  const int grid = dev.sms * (dev.max_threads_per_sm / kTPB);
+  const int grid = dev.grid_blocks(kTPB);
   ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, ctr, status);
   ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, ctr, status);

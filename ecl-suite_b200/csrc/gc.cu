@@ -32,7 +32,7 @@
 //    costs one poll, not a scan of the row.
 #include "csr_bins.cuh"
 #include "radix_sort.cuh"
-#include "runtime.cuh"
+#include "solvers.cuh"
 
 namespace ecl {
 namespace {
@@ -59,20 +59,41 @@ __device__ __forceinline__ bool gc_outranks(int du, unsigned hu, int u, int dv, 
   return u > v;
 }
 
+// Priority hash of vertex x: the reference hashes the vertex id; in a union
+// of graphs (vhash != nullptr) it is the hash of x's LOCAL id, precomputed.
+__device__ __forceinline__ unsigned gc_h(const unsigned* vhash, int x) {
+  return vhash ? __ldg(&vhash[x]) : ecl_hash((unsigned)x);
+}
+
 // 0: ignore (self-loop or invalid), 1: higher priority, 2: lower priority.
-__device__ __forceinline__ int gc_class(int u, int v, int dv, unsigned hv, int n, const int* nindex, Status* status) {
+__device__ __forceinline__ int gc_class(int u, int v, int dv, unsigned hv, int n, const int* nindex,
+                                        const unsigned* vhash, Status* status) {
   if ((unsigned)u >= (unsigned)n) {
     raise(status, ECL_ERR_BAD_GRAPH, u);
     return 0;
   }
   if (u == v) return 0;
   const int du = __ldg(&nindex[u + 1]) - __ldg(&nindex[u]);
-  return gc_outranks(du, ecl_hash((unsigned)u), u, dv, hv, v) ? 1 : 2;
+  return gc_outranks(du, gc_h(vhash, u), u, dv, hv, v) ? 1 : 2;
+}
+
+// vhash[v] = hash of v's local id in a union of graphs.
+__global__ void __launch_bounds__(kTPB) gc_union_hash(int n, const int* __restrict__ vbase, int ngraphs,
+                                                      unsigned* __restrict__ vhash) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    int lo = 0, hi = ngraphs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(&vbase[mid]) <= v) lo = mid;
+      else hi = mid - 1;
+    }
+    vhash[v] = ecl_hash((unsigned)(v - __ldg(&vbase[lo])));
+  }
 }
 
 __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ nl2,
-                                                int* __restrict__ hc, RowChunks rc,
+                                                int* __restrict__ hc, RowChunks rc, const unsigned* __restrict__ vhash,
                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -82,13 +103,13 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
     int beg = 0, end = 0;
     if (v < n) csr_row(nindex, v, m, beg, end, status);
     const int dv = end - beg;
-    const unsigned hv = ecl_hash((unsigned)v);
+    const unsigned hv = (v < n) ? gc_h(vhash, v) : 0u;
     int h = 0;
     if (dv > kBinChunk) push_row_chunks(rc, v, beg, end);
     if (v < n && dv <= kBinLane) {
       for (int i = beg; i < end; i++) {
         const int u = __ldg(&nlist[i]);
-        const int k = gc_class(u, v, dv, hv, n, nindex, status);
+        const int k = gc_class(u, v, dv, hv, n, nindex, vhash, status);
         if (k == 1) nl2[beg + h++] = u;
       }
     }
@@ -99,13 +120,13 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       const int wv = __shfl_sync(kFull, v, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      const unsigned whv = ecl_hash((unsigned)wv);
+      const unsigned whv = gc_h(vhash, wv);
       int wh = 0;
       for (int i0 = wbeg; i0 < wend; i0 += 32) {
         int k = 0, u = 0;
         if (i0 + lane < wend) {
           u = __ldg(&nlist[i0 + lane]);
-          k = gc_class(u, wv, wend - wbeg, whv, n, nindex, status);
+          k = gc_class(u, wv, wend - wbeg, whv, n, nindex, vhash, status);
         }
         const unsigned bh = __ballot_sync(kFull, k == 1);
         if (k == 1) nl2[wbeg + wh + __popc(bh & ((1u << lane) - 1))] = u;
@@ -120,6 +141,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
 __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ nl2,
                                                        int* __restrict__ hc, RowChunks rc,
+                                                       const unsigned* __restrict__ vhash,
                                                        Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -130,12 +152,12 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
     const int v = r.x;
     const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
     const int stop = min(r.y + kBinChunk, end);
-    const unsigned hv = ecl_hash((unsigned)v);
+    const unsigned hv = gc_h(vhash, v);
     for (int i0 = r.y; i0 < stop; i0 += 32) {
       int k = 0, u = 0;
       if (i0 + lane < stop) {
         u = __ldg(&nlist[i0 + lane]);
-        k = gc_class(u, v, end - beg, hv, n, nindex, status);
+        k = gc_class(u, v, end - beg, hv, n, nindex, vhash, status);
       }
       const unsigned bh = __ballot_sync(kFull, k == 1);
       int hbase = 0;
@@ -151,14 +173,14 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
 // sort breaks the remaining ties by descending id -- exactly the priority.
 __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ nindex,
                                                 unsigned long long* __restrict__ keys, int* __restrict__ vals,
-                                                GCCtl* __restrict__ ctl) {
+                                                const unsigned* __restrict__ vhash, GCCtl* __restrict__ ctl) {
   for (int base = (blockIdx.x * kTPB + threadIdx.x) & ~31; base < n; base += gridDim.x * kTPB) {
     const int i = base + (threadIdx.x & 31);
     bool big = false;
     if (i < n) {
       const int v = n - 1 - i;
       const unsigned deg = (unsigned)(__ldg(&nindex[v + 1]) - __ldg(&nindex[v]));
-      keys[i] = ~(((unsigned long long)deg << 32) | ecl_hash((unsigned)v));
+      keys[i] = ~(((unsigned long long)deg << 32) | gc_h(vhash, v));
       vals[i] = v;
       big = deg > (unsigned)kWarpRow;
     }
@@ -285,6 +307,7 @@ struct GCBufs {
   int* vals0;
   int* vals1;
   unsigned* sort_temp;
+  unsigned* vhash;
   int2* chunks;
 };
 
@@ -297,6 +320,7 @@ void gc_layout(Carve& c, int n, int m, GCBufs* b) {
   b->vals0 = c.take<int>((size_t)n);
   b->vals1 = c.take<int>((size_t)n);
   b->sort_temp = c.take<unsigned>(radix_temp_words((size_t)n));
+  b->vhash = c.take<unsigned>((size_t)n);
   b->chunks = c.take<int2>(row_chunk_capacity(m));
 }
 
@@ -307,6 +331,45 @@ size_t gc_workspace_bytes(int n, int m) {
   GCBufs b;
   gc_layout(c, n, m, &b);
   return c.bytes();
+}
+
+}  // namespace ecl
+
+namespace ecl {
+
+ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, const DeviceInfo& dev,
+                      cudaStream_t stream, const UnionInfo* uni, Marker mark) {
+  Carve c{ws};
+  GCBufs b;
+  gc_layout(c, g.n, g.m, &b);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
+    return ECL_ERR_CUDA;
+  const int coop_grid = dev.sms * occ;
+  const int grid = dev.grid_blocks(kTPB);
+  const RowChunks rc{b.chunks, &b.ctl->nchunks};
+  // key bits that vary: 32 hash bits + enough bits for any degree <= m
+  int degbits = 1;
+  while (degbits < 31 && ((long long)1 << degbits) <= (long long)g.m) degbits++;
+
+  if (cudaMemsetAsync(b.ctl, 0, sizeof(GCCtl), stream) != cudaSuccess) return ECL_ERR_CUDA;
+  if (cudaMemsetAsync(color, 0xff, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
+  const unsigned* vhash = nullptr;
+  if (uni && uni->vbase) {
+    ECL_LAUNCH(gc_union_hash, grid, kTPB, 0, stream, g.n, uni->vbase, uni->ngraphs, b.vhash);
+    vhash = b.vhash;
+  }
+  ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, vhash, status);
+  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, vhash, status);
+  mark();
+  ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
+  const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);
+  const int* order = in1 ? b.vals1 : b.vals0;
+  mark();
+  ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
+                                  status));
+  mark();
+  return ECL_OK;
 }
 
 }  // namespace ecl
@@ -324,38 +387,16 @@ extern "C" ecl_status ecl_gc(const ecl_graph_view* g, int32_t* color_out, ecl_op
   if (st != ECL_OK) return s.finish(st);
   int* color = s.output(color_out, (size_t)s.n);
   if (!color) return s.finish(ECL_ERR_OOM);
-  Carve c{s.ws};
-  GCBufs b;
-  gc_layout(c, s.n, s.m, &b);
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
-    return s.finish(ECL_ERR_CUDA);
-  const int coop_grid = s.dev.sms * occ;
-  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-  const RowChunks rc{b.chunks, &b.ctl->nchunks};
-  // key bits that vary: 32 hash bits + enough bits for any degree <= m
-  int degbits = 1;
-  while (degbits < 31 && ((long long)1 << degbits) <= (long long)s.m) degbits++;
-
+  GraphDev gd;
+  gd.n = s.n;
+  gd.m = s.m;
+  gd.nindex = s.nindex;
+  gd.nlist = s.nlist;
+  gd.flags = g->flags;
   s.start_timer();
-  if (cudaMemsetAsync(b.ctl, 0, sizeof(GCCtl), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  if (cudaMemsetAsync(color, 0xff, sizeof(int) * (size_t)s.n, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  ECL_LAUNCH(gc_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.nl2, b.hc, rc, s.status);
-  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.nl2, b.hc, rc, s.status);
-  s.mark();
-  ECL_LAUNCH(gc_keys, grid, kTPB, 0, s.stream, s.n, s.nindex, b.keys0, b.vals0, b.ctl);
-  const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, s.n, 0, 32 + degbits, b.sort_temp, s.stream);
-  const int* order = in1 ? b.vals1 : b.vals0;
-  s.mark();
-  int n_ = s.n;
-  const int* nindex_ = s.nindex;
-  void* args[] = {&n_, &nindex_, &b.nl2, &b.hc, &order, &color, &b.ctl, &s.status};
-  if (cudaLaunchCooperativeKernel((void*)gc_pull, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
-    return s.finish(ECL_ERR_CUDA);
-  count_launch();
-  s.mark();
+  st = gc_enqueue(gd, color, s.ws, s.status, s.dev, s.stream, nullptr, Marker{&s});
   s.stop_timer();
-  return s.finish();
+  return s.finish(st);
 }
 
 extern "C" ecl_status ecl_compute_gc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,

@@ -22,7 +22,7 @@
 //  * a self-loop (the reference spins forever on one: v never outranks
 //    itself) raises ECL_ERR_BAD_GRAPH when it is met; a sweep cap turns any
 //    other non-converging input into ECL_ERR_NO_CONVERGENCE.
-#include "runtime.cuh"
+#include "solvers.cuh"
 
 namespace ecl {
 namespace {
@@ -44,10 +44,25 @@ __device__ __forceinline__ unsigned mis_priority(int v, int degree, float avg, f
   return (unsigned)((res + res) | 1) & 0xffu;
 }
 
+// Graph of union vertex v: the last g with vbase[g] <= v (binary search).
+__device__ __forceinline__ int union_graph_of(const int* vbase, int ngraphs, int v) {
+  int lo = 0, hi = ngraphs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&vbase[mid]) <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// For a union of graphs (vbase != nullptr) every vertex uses ITS graph's
+// average degree and its local id, so each graph's bytes are exactly the ones
+// a solve of that graph alone computes.
 __global__ void __launch_bounds__(kTPB) mis_init(int n, int m, const int* __restrict__ nindex,
-                                                 unsigned* __restrict__ st4, int nwords, Status* __restrict__ status) {
-  const float avg = __fdiv_rn(__int2float_rn(m), __int2float_rn(n));
-  const float scaledavg = __fmul_rn(126.0f, avg);
+                                                 unsigned* __restrict__ st4, int nwords, const int* __restrict__ vbase,
+                                                 const float* __restrict__ avgs, int ngraphs,
+                                                 Status* __restrict__ status) {
+  const float avg1 = __fdiv_rn(__int2float_rn(m), __int2float_rn(n));
   for (int w = blockIdx.x * kTPB + threadIdx.x; w < nwords; w += gridDim.x * kTPB) {
     unsigned word = 0;
     for (int k = 0; k < 4; k++) {
@@ -56,7 +71,14 @@ __global__ void __launch_bounds__(kTPB) mis_init(int n, int m, const int* __rest
       if (v < n) {
         const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
         if (beg < 0 || end < beg || end > m) raise(status, ECL_ERR_BAD_GRAPH, v);
-        b = mis_priority(v, end - beg, avg, scaledavg);
+        float avg = avg1;
+        int local = v;
+        if (vbase) {
+          const int g = union_graph_of(vbase, ngraphs, v);
+          avg = __ldg(&avgs[g]);
+          local = v - __ldg(&vbase[g]);
+        }
+        b = mis_priority(local, end - beg, avg, __fmul_rn(126.0f, avg));
       }
       word |= b << (8 * k);
     }
@@ -215,6 +237,29 @@ size_t mis_workspace_bytes(int n, int m) {
 
 }  // namespace ecl
 
+namespace ecl {
+
+ecl_status mis_enqueue(const GraphDev& g, unsigned char* out, char* ws, Status* status, const DeviceInfo& dev,
+                       cudaStream_t stream, int max_sweeps, const UnionInfo* uni, Marker mark) {
+  Carve c{ws};
+  unsigned* st4;
+  mis_layout(c, g.n, &st4);
+  const int nwords = (g.n + 3) / 4;
+  const int grid = dev.grid_blocks(kTPB);
+  const int* vbase = uni ? uni->vbase : nullptr;
+  const float* avgs = uni ? uni->avg : nullptr;
+  const int ngraphs = uni ? uni->ngraphs : 0;
+  ECL_LAUNCH(mis_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, st4, nwords, vbase, avgs, ngraphs, status);
+  mark();
+  ECL_LAUNCH(mis_run, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, st4, status, max_sweeps);
+  mark();
+  ECL_LAUNCH(mis_emit, grid, kTPB, 0, stream, g.n, st4, out);
+  mark();
+  return ECL_OK;
+}
+
+}  // namespace ecl
+
 extern "C" ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status_out, ecl_opts* opts) {
   using namespace ecl;
   ecl_opts local{};
@@ -228,25 +273,20 @@ extern "C" ecl_status ecl_mis(const ecl_graph_view* g, uint8_t* status_out, ecl_
   if (st != ECL_OK) return s.finish(st);
   unsigned char* out = s.output(status_out, (size_t)s.n);
   if (!out) return s.finish(ECL_ERR_OOM);
-  Carve c{s.ws};
-  unsigned* st4;
-  mis_layout(c, s.n, &st4);
-  const int nwords = (s.n + 3) / 4;
-  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
+  GraphDev gd;
+  gd.n = s.n;
+  gd.m = s.m;
+  gd.nindex = s.nindex;
+  gd.nlist = s.nlist;
+  gd.flags = g->flags;
   // Warps sweep asynchronously (one may sweep many times while it waits on a
   // slower warp's vertex), so the cap is a fixed backstop against inputs that
   // cannot converge, not a per-graph bound.
   const int max_sweeps = opts->max_rounds > 0 ? opts->max_rounds : (1 << 22);
-
   s.start_timer();
-  ECL_LAUNCH(mis_init, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, st4, nwords, s.status);
-  s.mark();
-  ECL_LAUNCH(mis_run, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, st4, s.status, max_sweeps);
-  s.mark();
-  ECL_LAUNCH(mis_emit, grid, kTPB, 0, s.stream, s.n, st4, out);
-  s.mark();
+  st = mis_enqueue(gd, out, s.ws, s.status, s.dev, s.stream, max_sweeps, nullptr, Marker{&s});
   s.stop_timer();
-  return s.finish();
+  return s.finish(st);
 }
 
 extern "C" ecl_status ecl_compute_mis(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,

@@ -25,7 +25,7 @@
 #include <cooperative_groups.h>
 
 #include "grid_sync.cuh"
-#include "runtime.cuh"
+#include "solvers.cuh"
 
 namespace ecl {
 namespace {
@@ -95,10 +95,12 @@ __global__ void mst_init(int n, int* __restrict__ parent, u64* __restrict__ minv
 }
 
 // Threshold = the k-th smallest of kSamples sampled weights, k chosen so the
-// light pass keeps about 3n of the m entries (the reference's target,
-// ECL-MST_10-atomic.cu:450-459).  No filtering when edges/nodes < 4.
+// light pass keeps about light_factor * n of the m entries (the reference
+// aims at 3n, ECL-MST_10-atomic.cu:450-459; the batched engine's autotuner
+// may pick another factor -- the forest does not depend on it).  No
+// filtering when edges/nodes < 4.
 __global__ void __launch_bounds__(kSamples) mst_threshold(int n, int m, const int* __restrict__ eweight,
-                                                         MSTCtl* __restrict__ ctl) {
+                                                         MSTCtl* __restrict__ ctl, float light_factor) {
   __shared__ int s[kSamples];
   const int t = threadIdx.x;
   const bool filter = m > 0 && (m / n) >= 4;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(kSamples) mst_threshold(int n, int m, const in
   if (t == 0) {
     ctl->filter = filter ? 1 : 0;
     if (filter) {
-      const double frac = 3.0 * (double)n / (double)m;
+      const double frac = (double)light_factor * (double)n / (double)m;
       const int k = min(kSamples - 1, (int)(frac * kSamples));
       ctl->threshold = s[k];
     } else {
@@ -350,6 +352,48 @@ size_t mst_workspace_bytes(int n, int m) {
   return c.bytes();
 }
 
+ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Status* status, const DeviceInfo& dev,
+                       cudaStream_t stream, unsigned long long** total_dev, Marker mark) {
+  const bool sym = (g.flags & ECL_GRAPH_SYMMETRIC) != 0;
+  Carve c{ws};
+  MSTBufs b;
+  mst_layout(c, g.n, g.m, sym, &b);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mst_boruvka, kTPB, 0) != cudaSuccess || occ < 1)
+    return ECL_ERR_CUDA;
+  const int coop_grid = dev.sms * occ;
+  const int grid = dev.grid_blocks(kTPB);
+  if (total_dev) *total_dev = &b.ctl->total;
+  ECL_CUDA_TRY(cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), stream));
+  if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));
+  ECL_LAUNCH(mst_init, grid, kTPB, 0, stream, g.n, b.parent, b.minv);
+  if (g.m > 0) {
+    const float light = dev.mst_light_factor > 0.f ? dev.mst_light_factor : 3.0f;
+    ECL_LAUNCH(mst_threshold, 1, kSamples, 0, stream, g.n, g.m, g.eweight, b.ctl, light);
+    mark();
+    for (int pass = 0; pass < 2; pass++) {
+      if (pass == 0) {
+        ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
+                   b.cap, b.ctl, b.chunks, status);
+        ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
+                   b.ctl, b.chunks, status);
+      } else {
+        ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
+                   b.cap, b.ctl, b.chunks, status);
+        ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
+                   b.ctl, b.chunks, status);
+      }
+      mark();
+      ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.parent, b.minv,
+                                      in_mst, b.ctl, status));
+      mark();
+      // The heavy pass (pass 1) runs unconditionally: with no filter it finds
+      // no entry above the INT_MAX threshold and ends after one round.
+    }
+  }
+  return ECL_OK;
+}
+
 }  // namespace ecl
 
 extern "C" ecl_status ecl_mst(const ecl_graph_view* g, uint8_t* in_mst_out, uint64_t* total_weight, ecl_opts* opts) {
@@ -372,54 +416,23 @@ extern "C" ecl_status ecl_mst(const ecl_graph_view* g, uint8_t* in_mst_out, uint
   if (st != ECL_OK) return s.finish(st);
   unsigned char* in_mst = s.output(in_mst_out, (size_t)(s.m > 0 ? s.m : 1));
   if (!in_mst) return s.finish(ECL_ERR_OOM);
-  Carve c{s.ws};
-  MSTBufs b;
-  mst_layout(c, s.n, s.m, sym, &b);
-
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mst_boruvka, kTPB, 0) != cudaSuccess || occ < 1)
-    return s.finish(ECL_ERR_CUDA);
-  const int coop_grid = s.dev.sms * occ;
-  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
+  GraphDev gd;
+  gd.n = s.n;
+  gd.m = s.m;
+  gd.nindex = s.nindex;
+  gd.nlist = s.nlist;
+  gd.eweight = s.eweight;
+  gd.flags = g->flags;
+  u64* total_dev = nullptr;
   u64 hostTotal = 0;
-
   s.start_timer();
-  if (cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  if (s.m > 0 && cudaMemsetAsync(in_mst, 0, (size_t)s.m, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  ECL_LAUNCH(mst_init, grid, kTPB, 0, s.stream, s.n, b.parent, b.minv);
-  if (s.m > 0) {
-    ECL_LAUNCH(mst_threshold, 1, kSamples, 0, s.stream, s.n, s.m, s.eweight, b.ctl);
-    s.mark();
-    for (int pass = 0; pass < 2; pass++) {
-      if (pass == 0) {
-        ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, s.status);
-        ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, s.status);
-      } else {
-        ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, s.status);
-        ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, s.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, s.status);
-      }
-      s.mark();
-      int n_ = s.n;
-      int pass_ = pass;
-      void* args[] = {&n_, &pass_, &b.wlA, &b.wlB, &b.parent, &b.minv, &in_mst, &b.ctl, &s.status};
-      if (cudaLaunchCooperativeKernel((void*)mst_boruvka, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
-        return s.finish(ECL_ERR_CUDA);
-      count_launch();
-      s.mark();
-      // The heavy pass (pass 1) runs unconditionally: with no filter it finds
-      // no entry above the INT_MAX threshold and ends after one round.
-    }
-  }
+  st = mst_enqueue(gd, in_mst, s.ws, s.status, s.dev, s.stream, &total_dev, Marker{&s});
   s.stop_timer();
-  if (total_weight) {
-    if (cudaMemcpyAsync(&hostTotal, &b.ctl->total, sizeof(u64), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess)
-      return s.finish(ECL_ERR_CUDA);
+  if (st == ECL_OK && total_weight && total_dev) {
+    if (cudaMemcpyAsync(&hostTotal, total_dev, sizeof(u64), cudaMemcpyDeviceToHost, s.stream) != cudaSuccess)
+      st = ECL_ERR_CUDA;
   }
-  st = s.finish();
+  st = s.finish(st);
   if (total_weight) *total_weight = (st == ECL_OK) ? hostTotal : 0;
   return st;
 }

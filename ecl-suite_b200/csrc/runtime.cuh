@@ -39,12 +39,38 @@ void set_last_error_msg(const char* msg);
     ::ecl::count_launch();                                        \
   } while (0)
 
+// Cooperative (all blocks co-resident) launch through cudaLaunchKernelEx and
+// the cooperative launch attribute, which stream capture turns into a
+// cooperative CUDA-graph kernel node.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_cooperative(void (*kernel)(KArgs...), int grid, int block, cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  count_launch();
+  return e;
+}
+
 struct DeviceInfo {
   int device = -1;
   int sms = 0;
   int max_threads_per_sm = 0;
   int major = 0, minor = 0;
   size_t smem_optin = 0;
+  // Tunable launch knobs (0 = default), set by the batched engine's autotuner.
+  int blocks_per_sm = 0;
+  float mst_light_factor = 0.f;
+  // Grid of a grid-stride kernel with `tpb` threads per block: by default
+  // every SM filled to its thread limit.
+  int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }
 };
 // Properties of the current device (cached per device id).
 ecl_status current_device(DeviceInfo* info);

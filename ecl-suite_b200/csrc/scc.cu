@@ -24,7 +24,7 @@
 //  * the final labels are written by the same launch (label = in-max).
 #include "csr_bins.cuh"
 #include "grid_sync.cuh"
-#include "runtime.cuh"
+#include "solvers.cuh"
 
 namespace ecl {
 namespace {
@@ -319,6 +319,41 @@ size_t scc_workspace_bytes(int n, int m) {
 
 }  // namespace ecl
 
+namespace ecl {
+
+ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, const DeviceInfo& dev,
+                       cudaStream_t stream, int max_rounds, Marker mark) {
+  Carve c{ws};
+  SCCBufs b;
+  scc_layout(c, g.n, g.m, &b);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scc_solve, kTPB, 0) != cudaSuccess || occ < 1)
+    return ECL_ERR_CUDA;
+  const int coop_grid = dev.sms * occ;
+  const int grid = dev.grid_blocks(kTPB);
+  if (max_rounds <= 0 || max_rounds > b.max_rounds) max_rounds = b.max_rounds;
+
+  if (cudaMemsetAsync(b.ctl, 0, sizeof(SCCCtl), stream) != cudaSuccess) return ECL_ERR_CUDA;
+  if (cudaMemsetAsync(b.rounds, 0, sizeof(SCCRound) * (size_t)b.max_rounds, stream) != cudaSuccess)
+    return ECL_ERR_CUDA;
+  if (cudaMemsetAsync(b.hasin, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
+  if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
+  const RowChunks rc{b.chunks, b.nchunks};
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.hasin, b.hasout, b.imax, b.omax, rc,
+             status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.hasin, b.hasout, rc, status);
+  mark();
+  ECL_LAUNCH(scc_build, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.hasin, b.hasout, b.wlA, b.ctl);
+  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.hasin, b.hasout, b.wlA, b.ctl, rc);
+  mark();
+  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, b.wlA, b.wlB, b.imax, b.omax, label, b.ctl,
+                                  b.rounds, max_rounds, status));
+  mark();
+  return ECL_OK;
+}
+
+}  // namespace ecl
+
 extern "C" ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label_out, ecl_opts* opts) {
   using namespace ecl;
   ecl_opts local{};
@@ -329,39 +364,16 @@ extern "C" ecl_status ecl_scc(const ecl_graph_view* g, int32_t* label_out, ecl_o
   if (st != ECL_OK) return s.finish(st);
   int* label = s.output(label_out, (size_t)s.n);
   if (!label) return s.finish(ECL_ERR_OOM);
-  Carve c{s.ws};
-  SCCBufs b;
-  scc_layout(c, s.n, s.m, &b);
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scc_solve, kTPB, 0) != cudaSuccess || occ < 1)
-    return s.finish(ECL_ERR_CUDA);
-  const int coop_grid = s.dev.sms * occ;
-  const int grid = s.dev.sms * (s.dev.max_threads_per_sm / kTPB);
-  int max_rounds = b.max_rounds;
-  if (opts->max_rounds > 0 && opts->max_rounds < max_rounds) max_rounds = opts->max_rounds;
-
+  GraphDev gd;
+  gd.n = s.n;
+  gd.m = s.m;
+  gd.nindex = s.nindex;
+  gd.nlist = s.nlist;
+  gd.flags = g->flags;
   s.start_timer();
-  if (cudaMemsetAsync(b.ctl, 0, sizeof(SCCCtl), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  if (cudaMemsetAsync(b.rounds, 0, sizeof(SCCRound) * (size_t)b.max_rounds, s.stream) != cudaSuccess)
-    return s.finish(ECL_ERR_CUDA);
-  if (cudaMemsetAsync(b.hasin, 0, sizeof(int) * (size_t)s.n, s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), s.stream) != cudaSuccess) return s.finish(ECL_ERR_CUDA);
-  const RowChunks rc{b.chunks, b.nchunks};
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.hasout, b.imax, b.omax, rc,
-             s.status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.hasin, b.hasout, rc, s.status);
-  s.mark();
-  ECL_LAUNCH(scc_build, grid, kTPB, 0, s.stream, s.n, s.m, s.nindex, s.nlist, b.hasin, b.hasout, b.wlA, b.ctl);
-  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, s.stream, s.n, s.nindex, s.nlist, b.hasin, b.hasout, b.wlA, b.ctl, rc);
-  s.mark();
-  int n_ = s.n;
-  void* args[] = {&n_, &b.wlA, &b.wlB, &b.imax, &b.omax, &label, &b.ctl, &b.rounds, &max_rounds, &s.status};
-  if (cudaLaunchCooperativeKernel((void*)scc_solve, coop_grid, kTPB, args, 0, s.stream) != cudaSuccess)
-    return s.finish(ECL_ERR_CUDA);
-  count_launch();
-  s.mark();
+  st = scc_enqueue(gd, label, s.ws, s.status, s.dev, s.stream, opts->max_rounds, Marker{&s});
   s.stop_timer();
-  return s.finish();
+  return s.finish(st);
 }
 
 extern "C" ecl_status ecl_compute_scc(int32_t nodes, int32_t edges, const int32_t* nidx, const int32_t* nlist,

@@ -364,3 +364,97 @@ def _torch_dtype(name):
 
 def kernel_launches() -> int:
     return int(lib.ecl_kernel_launches())
+
+
+# ---- batched engine (include/ecl_batch.h) ------------------------------------------
+
+BATCH_CC, BATCH_MIS, BATCH_GC, BATCH_MST, BATCH_SCC = 0x1, 0x2, 0x4, 0x8, 0x10
+
+
+class Tune(C.Structure):
+    _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float)]
+
+
+_PB = C.c_void_p
+_sig("ecl_batch_create", C.c_int, [C.POINTER(C.c_void_p)])
+_sig("ecl_batch_destroy", None, [_PB])
+_sig("ecl_batch_add", C.c_int, [_PB, _PV])
+_sig("ecl_batch_add_mix", C.c_int, [_PB, _I32, _I32, _I32, _U64, _I32])
+_sig("ecl_batch_build", C.c_int, [_PB, C.c_uint32, C.c_int64, _VP])
+_sig("ecl_batch_run", C.c_int, [_PB, _PO])
+_sig("ecl_batch_tune", C.c_int, [_PB, _I32, C.POINTER(Tune)])
+_sig("ecl_batch_set_tune", C.c_int, [_PB, C.POINTER(Tune)])
+_sig("ecl_batch_graphs", C.c_int32, [_PB])
+_sig("ecl_batch_superbatches", C.c_int32, [_PB])
+_sig("ecl_batch_graph_size", C.c_int, [_PB, _I32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)])
+_sig("ecl_batch_graph_csr", C.c_int, [_PB, _I32, _VP, _VP, _VP])
+_sig("ecl_batch_result", C.c_int, [_PB, _I32, C.c_uint32, _VP, C.POINTER(C.c_uint64)])
+EXPORTED += ["ecl_batch_create", "ecl_batch_destroy", "ecl_batch_add", "ecl_batch_add_mix", "ecl_batch_build",
+             "ecl_batch_run", "ecl_batch_tune", "ecl_batch_set_tune", "ecl_batch_graphs", "ecl_batch_superbatches",
+             "ecl_batch_graph_size", "ecl_batch_graph_csr", "ecl_batch_result"]
+
+
+class Batch:
+    """Many graphs solved by one set of launches (one CUDA graph replay)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(lib.ecl_batch_create(C.byref(h)), "ecl_batch_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.ecl_batch_destroy(self.h)
+            self.h = None
+
+    def add(self, g: Graph):
+        v = g.view()
+        _check(lib.ecl_batch_add(self.h, C.byref(v)), "ecl_batch_add")
+
+    def add_mix(self, count, n_min=1000, n_max=200000, seed=5, weight_max=1 << 16):
+        _check(lib.ecl_batch_add_mix(self.h, count, n_min, n_max, seed, weight_max), "ecl_batch_add_mix")
+
+    def build(self, codes, max_entries=0, stream=None):
+        _check(lib.ecl_batch_build(self.h, codes, max_entries, stream), "ecl_batch_build")
+
+    def run(self):
+        o = Opts()
+        _check(lib.ecl_batch_run(self.h, C.byref(o)), "ecl_batch_run")
+        return o.elapsed_ms, bool(o.rounds)
+
+    def tune(self, trials=2):
+        t = Tune()
+        _check(lib.ecl_batch_tune(self.h, trials, C.byref(t)), "ecl_batch_tune")
+        return t.blocks_per_sm, t.mst_light_factor
+
+    @property
+    def graphs(self) -> int:
+        return int(lib.ecl_batch_graphs(self.h))
+
+    @property
+    def superbatches(self) -> int:
+        return int(lib.ecl_batch_superbatches(self.h))
+
+    def graph(self, i) -> Graph:
+        n, m = C.c_int32(), C.c_int32()
+        _check(lib.ecl_batch_graph_size(self.h, i, C.byref(n), C.byref(m)), "ecl_batch_graph_size")
+        ni = np.empty(n.value + 1, np.int32)
+        nl = np.empty(max(m.value, 1), np.int32)
+        ew = np.empty(max(m.value, 1), np.int32)
+        _check(lib.ecl_batch_graph_csr(self.h, i, ni.ctypes.data, nl.ctypes.data, ew.ctypes.data), "ecl_batch_graph_csr")
+        return Graph(ni, nl[: m.value], ew[: m.value], True)
+
+    def result(self, i, code):
+        n, m = C.c_int32(), C.c_int32()
+        _check(lib.ecl_batch_graph_size(self.h, i, C.byref(n), C.byref(m)), "ecl_batch_graph_size")
+        if code in (BATCH_CC, BATCH_SCC, BATCH_GC):
+            out = np.empty(n.value, np.int32)
+        elif code == BATCH_MIS:
+            out = np.empty(n.value, np.uint8)
+        else:
+            out = np.empty(max(m.value, 1), np.uint8)
+        tot = C.c_uint64(0)
+        _check(lib.ecl_batch_result(self.h, i, code, out.ctypes.data, C.byref(tot)), "ecl_batch_result")
+        if code == BATCH_MST:
+            return out[: m.value], int(tot.value)
+        return out
