@@ -38,7 +38,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["suite", "grid", "apsp", "batch"], default="suite")
+    p.add_argument("--workload", choices=["suite", "grid", "apsp", "batch", "serve"], default="suite")
+    p.add_argument("--serve-graphs", type=int, default=16)
     p.add_argument("--batch-count", type=int, default=4096)
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -246,6 +247,88 @@ def run_batch(args, rank, world, local_rank):
         print(json.dumps(line), flush=True)
 
 
+def run_serve(args, rank, world, local_rank):
+    """Served config: Poisson arrivals (seed 6) of CC/MIS/GC/MST/SCC requests
+    on a pool of resident seeded graphs (R-MAT or grid, n log-uniform in
+    [10k, 8M], edge factor 8-16, weights uniform in [1, 2^20)), admitted
+    against a 160 GB HBM budget; rates swept 10 - 10k req/s.  value =
+    graphs/s at the highest rate; p50/p99 latency per rate."""
+    import math
+
+    import numpy as np
+    import torch
+
+    import ecl_b200 as ecl
+
+    torch.cuda.set_device(local_rank)
+    rng = np.random.default_rng(6)
+    srv = ecl.Server(slots=8, hbm_budget_bytes=160 * 10**9)
+    t0 = time.perf_counter()
+    pool = []
+    for k in range(args.serve_graphs):
+        n = int(math.exp(rng.uniform(math.log(1e4), math.log(8e6))))
+        ef = int(rng.integers(8, 17))
+        if rng.random() < 0.5:
+            g = ecl.gen_rmat(max(1, round(math.log2(n))), ef, seed=600 + k, weight_seed=700 + k, weight_max=1 << 20)
+            kind = "rmat"
+        else:
+            r = max(1, int(math.sqrt(n)))
+            g = ecl.gen_grid(r, max(1, n // r), 0.0, seed=600 + k, weight_seed=700 + k, weight_max=1 << 20)
+            kind = "grid"
+        g.symmetric = True
+        pool.append((srv.add_graph(g), g.nodes, g.edges, kind))
+        print(f"serve: graph {k} {kind} n={g.nodes} m={g.edges}", file=sys.stderr, flush=True)
+    setup_s = time.perf_counter() - t0
+    codes = [ecl.CC, ecl.MIS, ecl.GC, ecl.MST, ecl.SCC]
+    names = {ecl.CC: "cc", ecl.MIS: "mis", ecl.GC: "gc", ecl.MST: "mst", ecl.SCC: "scc"}
+    sweep = []
+    l0 = ecl.kernel_launches()
+    # warm-up: every code on the largest graph (grows the device memory pool
+    # to its working size once) and on a small one
+    big = max(pool, key=lambda p: p[2])[0]
+    srv.run([(c, gid, 0.0, None) for c in codes for gid in (big, pool[0][0])])
+    clk = Clocks(local_rank)
+    clk.start()
+    for rate in (10, 100, 1000, 10000):
+        count = int(min(400, max(40, rate * 3)))
+        t = 0.0
+        reqs = []
+        for _ in range(count):
+            t += rng.exponential(1.0 / rate)
+            c = codes[int(rng.integers(0, 5))]
+            gid = pool[int(rng.integers(0, len(pool)))][0]
+            reqs.append((c, gid, t, None))
+        print(f"serve: rate {rate} req/s, {count} requests", file=sys.stderr, flush=True)
+        rc, arr, st = srv.run(reqs)
+        print(f"serve: rate {rate} done rc={rc} p50={st.p50_s*1e3:.2f} ms p99={st.p99_s*1e3:.2f} ms "
+              f"{st.graphs_per_s:.1f} graphs/s", file=sys.stderr, flush=True)
+        per = {}
+        for c in codes:
+            lat = sorted(arr[k].latency_s for k in range(count) if arr[k].code == c and arr[k].status == 0)
+            if lat:
+                per[names[c]] = {"p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                                 "n": len(lat)}
+        sweep.append({"rate_req_s": rate, "requests": count, "completed": st.completed, "failed": st.failed,
+                      "graphs_per_s": st.graphs_per_s, "p50_ms": 1e3 * st.p50_s, "p99_ms": 1e3 * st.p99_s,
+                      "mean_ms": 1e3 * st.mean_s, "max_in_flight": st.max_in_flight,
+                      "peak_gb": st.peak_bytes / 1e9, "per_code": per, "rc": rc})
+    clocks = clk.stop()
+    top = sweep[-1]
+    line = {
+        "metric": "graphs/s and p50/p99 latency of a served Poisson request stream (CC/MIS/GC/MST/SCC)",
+        "value": top["graphs_per_s"], "unit": "graphs/s", "n_gpus": world, "steps": len(sweep), "warmup": 1,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT / grid pool, seed 6)",
+        "config": {"workload": f"serve: {len(pool)} resident graphs, n log-uniform [10k, 8M], ef 8-16, "
+                               f"budget 160 GB, 8 slots", "graphs": [{"n": p[1], "m": p[2], "kind": p[3]} for p in pool],
+                   "resident_gb": sum(4 * (p[1] + 1) + 8 * p[2] for p in pool) / 1e9, "parallelism": f"replicas x{world}"},
+        "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": sweep, "setup_s": round(setup_s, 2),
+        "gpu_launches": int(ecl.kernel_launches() - l0), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -254,6 +337,8 @@ def run_ours(args, rank, world, local_rank):
 
     if args.workload == "batch":
         return run_batch(args, rank, world, local_rank)
+    if args.workload == "serve":
+        return run_serve(args, rank, world, local_rank)
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)

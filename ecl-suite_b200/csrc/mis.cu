@@ -13,8 +13,8 @@
 //    device-scope relaxed atomic on the word;
 //  * mis_init computes the priority bytes with the reference's fp32 formula
 //    using explicit round-to-nearest intrinsics (no contraction);
-//  * mis_run is ONE persistent launch: each warp sweeps its vertex groups
-//    until all are decided.  Lists of <= 32 entries are scanned by their own
+//  * mis_run is ONE persistent cooperative launch (all blocks co-resident):
+//    each warp sweeps its vertex groups until all are decided.  Lists of <= 32 entries are scanned by their own
 //    lane with an early exit at the first blocker; longer lists are scanned
 //    32 entries per step by the whole warp (two ballots per step); a joining
 //    vertex claims itself with one CAS, then clears its neighbours' bytes
@@ -22,6 +22,8 @@
 //  * a self-loop (the reference spins forever on one: v never outranks
 //    itself) raises ECL_ERR_BAD_GRAPH when it is met; a sweep cap turns any
 //    other non-converging input into ECL_ERR_NO_CONVERGENCE.
+#include <algorithm>
+
 #include "solvers.cuh"
 
 namespace ecl {
@@ -251,7 +253,14 @@ ecl_status mis_enqueue(const GraphDev& g, unsigned char* out, char* ws, Status* 
   const int ngraphs = uni ? uni->ngraphs : 0;
   ECL_LAUNCH(mis_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, st4, nwords, vbase, avgs, ngraphs, status);
   mark();
-  ECL_LAUNCH(mis_run, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, st4, status, max_sweeps);
+  // Warps of mis_run wait (by sweeping) for vertices owned by other warps,
+  // so all its blocks must be resident together: a cooperative launch
+  // guarantees that even when other solves share the GPU (server slots).
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mis_run, kTPB, 0) != cudaSuccess || occ < 1)
+    return ECL_ERR_CUDA;
+  ECL_CUDA_TRY(launch_cooperative(mis_run, dev.sms * std::min(occ, dev.max_threads_per_sm / kTPB), kTPB, stream, g.n,
+                                  g.m, g.nindex, g.nlist, st4, status, max_sweeps));
   mark();
   ECL_LAUNCH(mis_emit, grid, kTPB, 0, stream, g.n, st4, out);
   mark();

@@ -44,6 +44,16 @@ ecl_status current_device(DeviceInfo* info) {
     c.minor = p.minor;
     c.smem_optin = p.sharedMemPerBlockOptin;
     c.device = d;
+    // Workspaces come from the device's default memory pool (cudaMallocAsync).
+    // Its default release threshold (0) hands freed memory back to the driver
+    // at every synchronisation, so the next large workspace is mapped again;
+    // keep freed memory in the pool instead.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, d) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
   }
   if (c.major != 10) {
     set_last_error_msg("this library is built for sm_100a (B200) only");

@@ -458,3 +458,76 @@ class Batch:
         if code == BATCH_MST:
             return out[: m.value], int(tot.value)
         return out
+
+
+# ---- server (include/ecl_server.h) ---------------------------------------------------
+
+
+class ServerCfg(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("hbm_budget_bytes", C.c_uint64)]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("code", C.c_int32),
+        ("graph", C.c_int32),
+        ("arrival_s", C.c_double),
+        ("out", C.c_void_p),
+        ("total_weight", C.c_uint64),
+        ("latency_s", C.c_double),
+        ("queue_s", C.c_double),
+        ("status", C.c_int32),
+        ("slot", C.c_int32),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_int32),
+        ("failed", C.c_int32),
+        ("makespan_s", C.c_double),
+        ("graphs_per_s", C.c_double),
+        ("p50_s", C.c_double),
+        ("p99_s", C.c_double),
+        ("mean_s", C.c_double),
+        ("max_in_flight", C.c_int32),
+        ("peak_bytes", C.c_uint64),
+    ]
+
+
+_sig("ecl_server_create", C.c_int, [C.POINTER(ServerCfg), C.POINTER(C.c_void_p)])
+_sig("ecl_server_destroy", None, [C.c_void_p])
+_sig("ecl_server_add_graph", C.c_int, [C.c_void_p, _PV, C.POINTER(C.c_int32)])
+_sig("ecl_server_run", C.c_int, [C.c_void_p, C.POINTER(Request), C.c_int32, C.POINTER(ServerStats)])
+EXPORTED += ["ecl_server_create", "ecl_server_destroy", "ecl_server_add_graph", "ecl_server_run"]
+
+
+class Server:
+    """Continuous-batching server over resident graphs (see ecl_server.h).
+    Result buffers should be pinned host memory so copies stay asynchronous."""
+
+    def __init__(self, slots=8, hbm_budget_bytes=0):
+        cfg = ServerCfg(slots, hbm_budget_bytes)
+        h = C.c_void_p()
+        _check(lib.ecl_server_create(C.byref(cfg), C.byref(h)), "ecl_server_create")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.ecl_server_destroy(self.h)
+            self.h = None
+
+    def add_graph(self, g: Graph) -> int:
+        gid = C.c_int32()
+        v = g.view()
+        _check(lib.ecl_server_add_graph(self.h, C.byref(v), C.byref(gid)), "ecl_server_add_graph")
+        return int(gid.value)
+
+    def run(self, reqs):
+        """reqs: list of (code, graph_id, arrival_s, out_ptr_or_None)."""
+        arr = (Request * len(reqs))()
+        for k, (code, gid, t, out) in enumerate(reqs):
+            arr[k].code, arr[k].graph, arr[k].arrival_s, arr[k].out = code, gid, t, out
+        st = ServerStats()
+        rc = lib.ecl_server_run(self.h, arr, len(reqs), C.byref(st))
+        return rc, arr, st

@@ -5,7 +5,7 @@ import re
 
 from conftest import ROOT
 
-HEADERS = ["ecl_b200.h", "ecl_batch.h"]
+HEADERS = ["ecl_b200.h", "ecl_batch.h", "ecl_server.h"]
 
 
 def declared_functions():
