@@ -8,7 +8,9 @@
 // {(v, u) : u in list(v), u < v}.  That value does not depend on the schedule,
 // so any union-find with the same hooking rule reproduces it bit for bit.
 //
-// B200 design:
+// B200 design (graphs flagged ECL_GRAPH_SYMMETRIC take the sampling path
+// further down: link the first two entries of every list, find the giant
+// component, then skip every list inside it):
 //  * cc_init   - parent[v] = first smaller neighbour among the first
 //                kInitScan entries (one free hook per vertex).
 //  * cc_hook   - one pass over the vertices, 32 per warp.  Lists of <= 16
@@ -51,7 +53,8 @@ __device__ __forceinline__ bool cc_valid(int u, int n, Status* status) {
 
 struct CCCounters {
   int nchunks;
-  int pad[63];
+  int giant;  // root of the sampled largest component (symmetric path)
+  int pad[62];
 };
 
 // Root of v with path splitting.  Parent pointers only ever point at
@@ -195,10 +198,161 @@ __global__ void __launch_bounds__(kTPB) cc_flatten(int n, int* __restrict__ pare
   }
 }
 
-void cc_layout(Carve& c, int n, int m, CCCounters** ctr, int2** chunks) {
-  (void)n;
+// ---- symmetric graphs: sampling + giant-component skip ----------------------
+//
+// For a symmetric graph the components over the entries u < v are the plain
+// connected components, so every entry may be used in either direction
+// (Sutton, Ben-Nun and Barak, "Optimizing parallel graph connectivity
+// computation via subgraph sampling", IPDPS 2018).  Links still hook the
+// larger root under the smaller one, so the labels stay the minimum ids.
+
+constexpr int kSample = 2;  // list entries linked per vertex before the skip
+
+__global__ void __launch_bounds__(kTPB) cc_sample(int n, int m, const int* __restrict__ nindex,
+                                                  const int* __restrict__ nlist, int* __restrict__ parent,
+                                                  Status* __restrict__ status) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    int beg, end;
+    cc_row(nindex, v, m, beg, end);
+    const int stop = min(end, beg + kSample);
+    int rv = -1;
+    for (int i = beg; i < stop; i++) {
+      const int u = __ldg(&nlist[i]);
+      if (u == v || !cc_valid(u, n, status)) continue;
+      if (rv < 0) rv = cc_root(v, parent);
+      const int ru = cc_root(u, parent);
+      if (ru != rv) rv = cc_link(rv, ru, parent);
+    }
+  }
+}
+
+// One block: the most frequent root among 1024 sampled vertices.
+__global__ void __launch_bounds__(1024) cc_giant(int n, const int* __restrict__ parent, CCCounters* __restrict__ ctr) {
+  __shared__ int s[1024];
+  const int t = threadIdx.x;
+  s[t] = ld(&parent[ecl_hash((unsigned)t * 2654435761u + 97u) % (unsigned)n]);
+  __syncthreads();
+  for (int k = 2; k <= 1024; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int p = t ^ j;
+      if (p > t) {
+        const int a = s[t], b = s[p];
+        if ((a > b) == ((t & k) == 0)) {
+          s[t] = b;
+          s[p] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (t == 0) {
+    int best = s[0], run = 1, bestrun = 1;
+    for (int i = 1; i < 1024; i++) {
+      run = (s[i] == s[i - 1]) ? run + 1 : 1;
+      if (run > bestrun) {
+        bestrun = run;
+        best = s[i];
+      }
+    }
+    ctr->giant = best;
+  }
+}
+
+// Frozen membership of the sampled giant component (parent is flattened).
+__global__ void __launch_bounds__(kTPB) cc_mark_giant(int n, const int* __restrict__ parent,
+                                                      const CCCounters* __restrict__ ctr,
+                                                      unsigned char* __restrict__ ing) {
+  const int gr = ctr->giant;
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) ing[v] = parent[v] == gr;
+}
+
+// Remaining entries of vertices outside the giant component.  An entry is
+// linked when u < v (the other direction is handled from u) or when u is in
+// the giant component (u skips its list entirely).
+__device__ __forceinline__ bool cc_rest_wanted(int u, int v, const unsigned char* ing) {
+  return u != v && (u < v || __ldg(&ing[u]));
+}
+
+__global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restrict__ nindex,
+                                                const int* __restrict__ nlist, int* __restrict__ parent,
+                                                const unsigned char* __restrict__ ing, int2* __restrict__ chunks,
+                                                CCCounters* __restrict__ ctr, Status* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  for (int base = warp * 32; base < n; base += nwarps * 32) {
+    const int v = base + lane;
+    int beg = 0, end = 0;
+    if (v < n && !__ldg(&ing[v])) {
+      cc_row(nindex, v, m, beg, end);
+      beg = min(end, beg + kSample);  // the first entries were linked by cc_sample
+    }
+    const int deg = end - beg;
+    if (deg > kChunk) {
+      const int nc = (deg + kChunk - 1) / kChunk;
+      const int at = fetch_add(&ctr->nchunks, nc);
+      for (int c = 0; c < nc; c++) chunks[at + c] = make_int2(v, beg + c * kChunk);
+    } else if (deg > 0 && deg <= kLaneMax) {
+      int rv = -1;
+      for (int i = beg; i < end; i++) {
+        const int u = __ldg(&nlist[i]);
+        if (cc_valid(u, n, status) && cc_rest_wanted(u, v, ing)) {
+          if (rv < 0) rv = cc_root(v, parent);
+          const int ru = cc_root(u, parent);
+          if (ru != rv) rv = cc_link(rv, ru, parent);
+        }
+      }
+    }
+    unsigned mid = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
+    while (mid) {
+      const int who = __ffs(mid) - 1;
+      mid &= mid - 1;
+      const int wv = __shfl_sync(kFull, v, who);
+      const int wbeg = __shfl_sync(kFull, beg, who);
+      const int wend = __shfl_sync(kFull, end, who);
+      int rv = -1;
+      for (int i = wbeg + lane; i < wend; i += 32) {
+        const int u = __ldg(&nlist[i]);
+        if (cc_valid(u, n, status) && cc_rest_wanted(u, wv, ing)) {
+          if (rv < 0) rv = cc_root(wv, parent);
+          const int ru = cc_root(u, parent);
+          if (ru != rv) rv = cc_link(rv, ru, parent);
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restrict__ nindex,
+                                                       const int* __restrict__ nlist, int* __restrict__ parent,
+                                                       const unsigned char* __restrict__ ing,
+                                                       const int2* __restrict__ chunks,
+                                                       const CCCounters* __restrict__ ctr, Status* __restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  const int total = ctr->nchunks;
+  for (int c = warp; c < total; c += nwarps) {
+    const int2 rec = chunks[c];
+    const int v = rec.x;
+    const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
+    int rv = -1;
+    for (int i = rec.y + lane; i < end; i += 32) {
+      const int u = __ldg(&nlist[i]);
+      if (cc_valid(u, n, status) && cc_rest_wanted(u, v, ing)) {
+        if (rv < 0) rv = cc_root(v, parent);
+        const int ru = cc_root(u, parent);
+        if (ru != rv) rv = cc_link(rv, ru, parent);
+      }
+    }
+  }
+}
+
+void cc_layout(Carve& c, int n, int m, CCCounters** ctr, int2** chunks, unsigned char** ing = nullptr) {
   *ctr = c.take<CCCounters>(1);
   *chunks = c.take<int2>((size_t)(2 * (m / kChunk) + 2));
+  unsigned char* g = c.take<unsigned char>((size_t)n);
+  if (ing) *ing = g;
 }
 
 }  // namespace
@@ -220,9 +374,25 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   Carve c{ws};
   CCCounters* ctr;
   int2* chunks;
-  cc_layout(c, g.n, g.m, &ctr, &chunks);
+  unsigned char* ing;
+  cc_layout(c, g.n, g.m, &ctr, &chunks, &ing);
   const int grid = dev.grid_blocks(kTPB);
   ECL_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(CCCounters), stream));
+  if (g.flags & ECL_GRAPH_SYMMETRIC) {
+    ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
+    ECL_LAUNCH(cc_sample, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
+    ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
+    ECL_LAUNCH(cc_giant, 1, 1024, 0, stream, g.n, parent, ctr);
+    ECL_LAUNCH(cc_mark_giant, grid, kTPB, 0, stream, g.n, parent, ctr, ing);
+    mark();
+    ECL_LAUNCH(cc_rest, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, ing, chunks, ctr, status);
+    mark();
+    ECL_LAUNCH(cc_rest_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, ing, chunks, ctr, status);
+    mark();
+    ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
+    mark();
+    return ECL_OK;
+  }
   ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
   mark();
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, ctr, status);

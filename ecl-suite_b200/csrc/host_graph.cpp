@@ -224,6 +224,80 @@ ecl_status ecl_graph_validate(const ecl_graph_view* g, int32_t require_symmetric
   return fwd == rev ? ECL_OK : ECL_ERR_BAD_GRAPH;
 }
 
+ecl_status ecl_graph_from_mm(const char* path, int32_t symmetrise, ecl_graph* out) {
+  if (!path || !out) return ECL_ERR_INVALID_ARG;
+  memset(out, 0, sizeof(*out));
+  FILE* f = fopen(path, "rt");
+  if (!f) return ECL_ERR_IO;
+  char line[1024];
+  if (!fgets(line, sizeof(line), f)) {
+    fclose(f);
+    return ECL_ERR_IO;
+  }
+  // banner checks of scripts/mm2ecl_real.cpp:63-72
+  if (!strstr(line, "%%MatrixMarket") || !strstr(line, "matrix") || !strstr(line, "coordinate") ||
+      (!strstr(line, "general") && !strstr(line, "symmetric")) ||
+      (!strstr(line, "integer") && !strstr(line, "pattern") && !strstr(line, "real"))) {
+    fclose(f);
+    return ECL_ERR_BAD_GRAPH;
+  }
+  const bool intw = strstr(line, "integer") != nullptr, realw = strstr(line, "real") != nullptr;
+  bool got = false;
+  while (fgets(line, sizeof(line), f)) {
+    if (line[0] != '%') {
+      got = true;
+      break;
+    }
+  }
+  int nodes = 0, cols = 0;
+  long long nnz = -1;
+  if (!got || sscanf(line, "%d %d %lld", &nodes, &cols, &nnz) != 3 || nodes < 1 || nnz < 0 || nodes != cols ||
+      nnz > INT32_MAX) {
+    fclose(f);
+    return ECL_ERR_BAD_GRAPH;
+  }
+  struct Entry {
+    int s, d;
+    double w;
+    bool operator<(const Entry& o) const { return s != o.s ? s < o.s : (d != o.d ? d < o.d : w < o.w); }
+  };
+  std::vector<Entry> e;
+  e.reserve((size_t)nnz * (symmetrise ? 2 : 1));
+  for (long long k = 0; k < nnz; k++) {
+    int s_ = 0, d_ = 0;
+    double w = 0;
+    const int want = (intw || realw) ? 3 : 2;
+    const int got_ = (want == 3) ? fscanf(f, "%d %d %lf", &s_, &d_, &w) : fscanf(f, "%d %d", &s_, &d_);
+    if (got_ != want || s_ < 1 || s_ > nodes || d_ < 1 || d_ > nodes) {
+      fclose(f);
+      return ECL_ERR_BAD_GRAPH;
+    }
+    e.push_back(Entry{s_ - 1, d_ - 1, w});
+    if (symmetrise && s_ != d_) e.push_back(Entry{d_ - 1, s_ - 1, w});
+  }
+  fclose(f);
+  if (e.size() > (size_t)INT32_MAX) return ECL_ERR_UNSUPPORTED;
+  std::sort(e.begin(), e.end());
+  const int m = (int)e.size();
+  out->nodes = nodes;
+  out->edges = m;
+  out->nindex = (int32_t*)calloc((size_t)nodes + 1, sizeof(int32_t));
+  out->nlist = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max(m, 1));
+  if (intw || realw) out->eweight = (int32_t*)malloc(sizeof(int32_t) * (size_t)std::max(m, 1));
+  if (!out->nindex || !out->nlist || ((intw || realw) && !out->eweight)) {
+    ecl_graph_free(out);
+    return ECL_ERR_OOM;
+  }
+  for (int i = 0; i < m; i++) {
+    out->nindex[e[i].s + 1] = i + 1;
+    out->nlist[i] = e[i].d;
+    if (intw) out->eweight[i] = (int32_t)e[i].w;
+    if (realw) out->eweight[i] = (int32_t)(e[i].w * 100);
+  }
+  for (int i = 1; i <= nodes; i++) out->nindex[i] = std::max(out->nindex[i - 1], out->nindex[i]);  // empty rows
+  return ECL_OK;
+}
+
 ecl_status ecl_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
                         int32_t symmetrise, uint64_t weight_seed, int32_t weight_max, ecl_graph* out) {
   if (!out || scale < 1 || scale > 30 || edge_factor < 1) return ECL_ERR_INVALID_ARG;

@@ -219,6 +219,15 @@ ecl_status ecl_graph_write(const char* path, const ecl_graph* g);
 /* freeECLgraph (ECLgraph.h:94-102). */
 void ecl_graph_free(ecl_graph* g);
 
+/* MatrixMarket "coordinate" file -> ECLgraph, with the semantics of the
+ * reference's converter (scripts/mm2ecl_real.cpp:50-184): square matrices,
+ * general or symmetric, pattern / integer / real; entries sorted by (row,
+ * column), 1-based ids made 0-based, real weights stored as (int)(w * 100),
+ * rows without entries get empty lists.  Like the reference, a "symmetric"
+ * file is NOT mirrored unless symmetrise != 0; then every off-diagonal entry
+ * (i, j) also yields (j, i) with the same weight. */
+ecl_status ecl_graph_from_mm(const char* path, int32_t symmetrise, ecl_graph* out);
+
 /* Host-side CSR checks.  require_symmetric / forbid_self_loops add those
  * checks (O(edges log deg)); returns ECL_OK or ECL_ERR_BAD_GRAPH. */
 ecl_status ecl_graph_validate(const ecl_graph_view* g, int32_t require_symmetric, int32_t forbid_self_loops);
