@@ -27,14 +27,17 @@ __global__ void __launch_bounds__(kThreads) rs_histogram(const unsigned long lon
   counts[(size_t)threadIdx.x * tiles + t] = h[threadIdx.x];
 }
 
-// Exclusive scan of counts[0..len) in place, one block of 1024 threads.
-__global__ void __launch_bounds__(1024) rs_scan(unsigned* __restrict__ counts, int len) {
+// Exclusive scan of each digit's row counts[d * tiles .. (d+1) * tiles) in
+// place (one block per digit); rowsum[d] = the row's total.
+__global__ void __launch_bounds__(1024) rs_scan_rows(unsigned* __restrict__ counts, int tiles,
+                                                    unsigned* __restrict__ rowsum) {
   __shared__ unsigned part[1024];
-  const int per = (len + 1023) / 1024;
+  unsigned* row = counts + (size_t)blockIdx.x * tiles;
+  const int per = (tiles + 1023) / 1024;
   const int b = threadIdx.x * per;
-  const int e = min(len, b + per);
+  const int e = min(tiles, b + per);
   unsigned s = 0;
-  for (int i = b; i < e; i++) s += counts[i];
+  for (int i = b; i < e; i++) s += row[i];
   part[threadIdx.x] = s;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {
@@ -45,16 +48,32 @@ __global__ void __launch_bounds__(1024) rs_scan(unsigned* __restrict__ counts, i
   }
   unsigned run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
   for (int i = b; i < e; i++) {
-    const unsigned c = counts[i];
-    counts[i] = run;
+    const unsigned c = row[i];
+    row[i] = run;
     run += c;
   }
+  if (threadIdx.x == 1023) rowsum[blockIdx.x] = part[1023];
+}
+
+// Exclusive scan of the 256 row totals in place: the base of each digit.
+__global__ void __launch_bounds__(256) rs_scan_digits(unsigned* __restrict__ rowsum) {
+  __shared__ unsigned part[256];
+  part[threadIdx.x] = rowsum[threadIdx.x];
+  __syncthreads();
+  for (int off = 1; off < 256; off <<= 1) {
+    const unsigned add = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += add;
+    __syncthreads();
+  }
+  rowsum[threadIdx.x] = threadIdx.x ? part[threadIdx.x - 1] : 0u;
 }
 
 __global__ void __launch_bounds__(kThreads) rs_scatter(const unsigned long long* __restrict__ kin,
                                                        const int* __restrict__ vin, unsigned long long* __restrict__ kout,
                                                        int* __restrict__ vout, int n, int shift,
-                                                       const unsigned* __restrict__ offsets, int tiles) {
+                                                       const unsigned* __restrict__ offsets,
+                                                       const unsigned* __restrict__ digitbase, int tiles) {
   __shared__ unsigned wcount[kWarps][256];  // per-warp digit counts, then per-warp bases
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = blockIdx.x;
@@ -70,7 +89,7 @@ __global__ void __launch_bounds__(kThreads) rs_scatter(const unsigned long long*
   // 2. base of each (warp, digit) = tile offset + counts of earlier warps
   {
     const int d = threadIdx.x;  // 256 threads, one digit each
-    unsigned run = offsets[(size_t)d * tiles + t];
+    unsigned run = digitbase[d] + offsets[(size_t)d * tiles + t];
     for (int w = 0; w < kWarps; w++) {
       const unsigned c = wcount[w][d];
       wcount[w][d] = run;
@@ -116,9 +135,11 @@ bool radix_sort_pairs(unsigned long long* k0, int* v0, unsigned long long* k1, i
     const int* vi = flip ? v1 : v0;
     unsigned long long* ko = flip ? k0 : k1;
     int* vo = flip ? v0 : v1;
+    unsigned* digitbase = temp + (size_t)256 * tiles;
     ECL_LAUNCH(rs_histogram, tiles, kThreads, 0, stream, ki, n, shift, temp, tiles);
-    ECL_LAUNCH(rs_scan, 1, 1024, 0, stream, temp, 256 * tiles);
-    ECL_LAUNCH(rs_scatter, tiles, kThreads, 0, stream, ki, vi, ko, vo, n, shift, temp, tiles);
+    ECL_LAUNCH(rs_scan_rows, 256, 1024, 0, stream, temp, tiles, digitbase);
+    ECL_LAUNCH(rs_scan_digits, 1, 256, 0, stream, digitbase);
+    ECL_LAUNCH(rs_scatter, tiles, kThreads, 0, stream, ki, vi, ko, vo, n, shift, temp, digitbase, tiles);
     flip = !flip;
   }
   return flip;

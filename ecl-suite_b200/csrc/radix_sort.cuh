@@ -1,7 +1,8 @@
 // Stable LSD radix sort of (uint64 key, int32 value) pairs, 8-bit digits.
 //
-// One pass = three launches: per-tile digit histograms, one exclusive scan
-// over the digit-major histogram table, and a stable scatter.  The scatter
+// One pass = four launches: per-tile digit histograms, a per-digit-row scan
+// of the digit-major histogram table, a scan of the 256 row totals, and a
+// stable scatter.  The scatter
 // ranks keys inside a tile warp by warp (warp w of a tile takes the w-th
 // slice of it): __match_any_sync groups the lanes holding the same digit, a
 // shared-memory table gives every warp its base per digit, so equal digits
