@@ -123,6 +123,11 @@ def phase_bytes(code, phase, n, m):
         ("cc", 1): csr + 4 * n,                    # hook: CSR + parent
         ("cc", 2): 4 * m // 8,                     # chunks: hub entries (upper bound share)
         ("cc", 3): 8 * n,                          # flatten: parent read + write
+        # symmetric path: 2 sampled entries per vertex, compressions, giant-membership bytes
+        ("cc_sym", 0): 4 * (n + 1) + 8 * n + 4 * n + 16 * n + n,
+        ("cc_sym", 1): 4 * (n + 1) + n,            # rest: rows + membership (giant rows skipped)
+        ("cc_sym", 2): 4 * m // 8,
+        ("cc_sym", 3): 8 * n,
         ("mis", 0): 4 * (n + 1) + n,
         ("mis", 1): csr + n,
         ("mis", 2): 2 * n,
@@ -143,6 +148,7 @@ def phase_bytes(code, phase, n, m):
 
 PHASE_NAMES = {
     "cc": ["cc_init", "cc_hook", "cc_chunks", "cc_flatten"],
+    "cc_sym": ["cc_init+sample+giant", "cc_rest", "cc_rest_chunks", "cc_flatten"],
     "mis": ["mis_init", "mis_run", "mis_emit"],
     "gc": ["gc_init+chunks", "gc_keys+radix_sort", "gc_pull"],
     "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
@@ -150,6 +156,11 @@ PHASE_NAMES = {
     "scc": ["scc_mark+chunks", "scc_build+chunks", "scc_solve"],
     "apsp": ["apsp_fill+edges", "apsp_panels+update"],
 }
+
+
+def phase_code(code, g):
+    """Phase table of a solve: symmetric graphs take CC's sampling path."""
+    return "cc_sym" if code == "cc" and getattr(g, "symmetric", False) else code
 
 
 # ---------------------------------------------------------------- our arm
@@ -351,11 +362,11 @@ def run_ours(args, rank, world, local_rank):
         wl_name = (f"rmat{args.scale}-suite: CC+MIS+GC+MST on symmetrised R-MAT-{args.scale} "
                    f"(n={sym.nodes}, m={sym.edges}), SCC on directed R-MAT-{args.scale} (m={dirg.edges})")
     elif args.workload == "grid":
-        g = ecl.gen_grid(1024, 1024, 0.05, seed=1)
+        g = grid_graph(ecl)
         jobs = [("cc", g)]
         wl_name = f"grid1024-cc: CC on 1024x1024 grid, 5% deleted (n={g.nodes}, m={g.edges})"
     else:
-        g = ecl.gen_er(8192, 0.001, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+        g = apsp_graph(ecl)
         jobs = [("apsp", g)]
         wl_name = f"er8192-apsp: blocked FW on ER n=8192 p=0.001 (m={g.edges})"
 
@@ -404,7 +415,7 @@ def run_ours(args, rank, world, local_rank):
             if timed:
                 per_code_ms[code] += ms
                 for i in range(o.nphases):
-                    key = (code, i)
+                    key = (phase_code(code, g), i)
                     phase_tot[key] = phase_tot.get(key, 0.0) + o.phase_ms[i]
             tot += ms
         return tot
@@ -426,12 +437,16 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.barrier()
     clocks = clk.stop()
 
-    edges_step = sum(g.edges for _, g in jobs)
+    is_apsp = jobs[0][0] == "apsp"
+    # units of one step: CSR entries (edges/s, as the reference prints), or
+    # n^3 relaxations for APSP (updates/s)
+    units_step = float(jobs[0][1].nodes) ** 3 if is_apsp else sum(g.edges for _, g in jobs)
+    unit = "updates/s" if is_apsp else "edges/s"
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * edges_step * args.steps / (total_ms / 1e3)
+    value = world * units_step * args.steps / (total_ms / 1e3)
     ms_per_step = total_ms / args.steps
 
     # dominant kernel phase and its roofline
@@ -440,7 +455,7 @@ def run_ours(args, rank, world, local_rank):
     roof = None
     if dom is not None and jobs[0][0] != "apsp":
         (code, idx), tot = dom
-        g = dict(jobs)[code]
+        g = {phase_code(c, gg): gg for c, gg in jobs}[code]
         avg_ms = tot / args.steps
         byts = phase_bytes(code, idx, g.nodes, g.edges)
         ach = byts / (avg_ms / 1e3) / 1e9
@@ -455,14 +470,19 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": traffic, "algorithmic_bytes": byts, "avg_ms": round(avg_ms, 4),
                 "share": round(tot / sum(phase_tot.values()), 3), "peak_source": pk.get("source")}
     elif dom is not None:
-        (code, idx), tot = dom
-        g = dict(jobs)[code]
-        n = g.nodes
-        avg_ms = tot / args.steps
-        ops = 2.0 * n ** 3  # one add + one min per update
-        roof = {"bound": "int32", "kernel": "apsp_panels+apsp_update", "achieved": round(ops / (avg_ms / 1e3) / 1e12, 3),
-                "peak": None, "unit": "Tops/s", "frac": None, "traffic": None, "avg_ms": round(avg_ms, 3),
-                "note": "INT32 add+min (2 ops per update; one DPX viaddmin instruction)"}
+        n = jobs[0][1].nodes
+        N = (n + 127) // 128 * 128
+        avg_ms = per_code_ms["apsp"] / args.steps
+        ops = 2.0 * float(N) ** 3  # one add + one min per update of the padded N x N closure
+        peak_dpx = ecl.minplus_peak(0) / 1e12
+        peak_sep = ecl.minplus_peak(1) / 1e12
+        ach = ops / (avg_ms / 1e3) / 1e12
+        roof = {"bound": "int32", "kernel": "apsp_panels+apsp_update", "achieved": round(ach, 3),
+                "peak": round(peak_dpx, 3), "unit": "Tops/s", "frac": round(ach / peak_dpx, 4), "traffic": None,
+                "avg_ms": round(avg_ms, 3), "peak_source": "measured in this run: ecl_minplus_peak(0), DPX add-min "
+                "throughput over a full wave (MEASURED_PEAKS.json has no integer peak)",
+                "peak_add_then_min": round(peak_sep, 3),
+                "note": "2 integer ops (add + min) per update of the padded N^3 closure, N = ceil(n/128)*128"}
 
     # end to end through the C ABI with pinned host buffers
     e2e = None
@@ -517,23 +537,30 @@ def run_ours(args, rank, world, local_rank):
             t = torch.tensor([e_ms], device=dev)
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             e_ms = float(t.item())
-        e2e = {"value": world * edges_step * args.e2e_steps / (e_ms / 1e3), "unit": "edges/s",
+        e2e = {"value": world * units_step * args.e2e_steps / (e_ms / 1e3), "unit": unit,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                "ms_per_step": e_ms / args.e2e_steps}
 
     cpu = None
-    if rank == 0 and world == 1 and args.workload == "suite":
-        cpu = cpu_baseline(ecl, scale=min(args.scale, 21))
+    if rank == 0 and world == 1:
+        if args.workload == "suite":
+            cpu = cpu_baseline(ecl, scale=min(args.scale, 21))
+        elif args.workload == "grid":
+            cpu = cpu_baseline_grid(ecl)
+        else:
+            cpu = cpu_baseline_apsp(ecl)
 
     per_code = {c: {"edges": g.edges, "ms": per_code_ms[c] / args.steps,
                     "edges_per_s": g.edges / (per_code_ms[c] / args.steps / 1e3)} for c, g in jobs}
     phases = {f"{PHASE_NAMES[c][i]}": round(v / args.steps, 4) for (c, i), v in sorted(phase_tot.items())}
+    metric = ("updates/s (n^3 / compute time of the blocked Floyd-Warshall closure; inputs resident)" if is_apsp else
+              "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)")
     line = {
-        "metric": "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)",
-        "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "metric": metric,
+        "value": value, "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic (seeded generators: R-MAT / grid / Erdos-Renyi)",
-        "config": {"workload": wl_name, "l2": "256 MiB write before every solve; CSR 513 MB > L2",
+        "config": {"workload": wl_name, "l2": "256 MiB write (> 126 MB L2) before every solve",
                    "parallelism": f"replicas x{world}"},
         "per_code": per_code, "phase_ms": phases, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks,
@@ -559,6 +586,8 @@ def _ref():
     r = C.CDLL(p)
     r.eclref_mst_cpu.restype = C.c_double
     r.eclref_mst_gpu.restype = C.c_double
+    r.eclref_apsp_gpu.restype = C.c_double
+    r.eclref_apsp_cpu.restype = C.c_double
     r.eclref_cc_device.restype = C.c_float
     r.eclref_mis_device.restype = C.c_float
     r.eclref_gc_device.restype = C.c_float
@@ -613,6 +642,89 @@ def cpu_baseline(ecl, scale):
             "per_code_kind": kinds}
 
 
+def grid_graph(ecl):
+    return ecl.gen_grid(1024, 1024, 0.05, seed=1)
+
+
+def apsp_graph(ecl, n=8192):
+    # ER with the same expected degree as n=8192, p=0.001 (about 8.2)
+    return ecl.gen_er(n, 0.001 * 8192 / n, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+
+
+def cpu_grid_once(g, orc):
+    t0 = time.perf_counter()
+    orc.cc(g)
+    return g.edges, time.perf_counter() - t0
+
+
+def cpu_baseline_grid(ecl):
+    orc = _orc()
+    g = grid_graph(ecl)
+    e, t = 0, 0.0
+    while t < 2.0:
+        de, dt = cpu_grid_once(g, orc)
+        e, t = e + de, t + dt
+    return {"value": e / t, "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"the full 1024x1024 grid, serial C oracle CC (the reference has no CPU CC solver), {t:.1f} s"}
+
+
+APSP_CPU_N = 2048  # sample size for the serial O(n^3) CPU closure
+
+
+def cpu_apsp_once(g, orc, ref):
+    """One serial closure on the host: the reference's own FW_cpu
+    (ECL-APSP-atomic.cu:533) when oracle/_ref is built, else the C oracle."""
+    import numpy as np
+
+    if ref is not None:
+        out = np.zeros((g.nodes, g.nodes), np.int32)
+        P = lambda a: C.c_void_p(a.ctypes.data)
+        t0 = time.perf_counter()
+        ref.eclref_apsp_cpu(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), P(out))
+        return float(g.nodes) ** 3, time.perf_counter() - t0, "reference"
+    t0 = time.perf_counter()
+    orc.apsp(g)
+    return float(g.nodes) ** 3, time.perf_counter() - t0, "port"
+
+
+def cpu_baseline_apsp(ecl):
+    g = apsp_graph(ecl, APSP_CPU_N)
+    u, t, kind = cpu_apsp_once(g, _orc(), _ref())
+    return {"value": u / t, "unit": "updates/s", "cores": 1, "kind": kind,
+            "sample": f"one serial closure on an ER graph with n={APSP_CPU_N} (same expected degree and weights), "
+                      f"{'reference FW_cpu' if kind == 'reference' else 'C oracle'}, {t:.1f} s"}
+
+
+def reference_gpu_grid(g):
+    import torch
+
+    ref = _ref()
+    if ref is None or not torch.cuda.is_available():
+        return None
+    P = lambda t: C.c_void_p(t.data_ptr())
+    ni, nl = torch.from_numpy(g.nindex).cuda(), torch.from_numpy(g.nlist).cuda()
+    st = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
+    wl = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
+    ms = min(ref.eclref_cc_device(g.nodes, P(ni), P(nl), P(st), P(wl)) for _ in range(5))
+    return {"value": g.edges / (ms / 1e3), "unit": "edges/s", "per_code": {"cc": {"ms": ms}},
+            "note": "reference race-free CUDA build (nvcc -O3 sm_100a), same graph, its own timed region"}
+
+
+def reference_gpu_apsp(g):
+    import numpy as np
+    import torch
+
+    ref = _ref()
+    if ref is None or not torch.cuda.is_available():
+        return None
+    upper = (g.nodes + 63) // 64 * 64
+    out = np.zeros((upper, upper), np.int32)
+    Q = lambda a: C.c_void_p(a.ctypes.data)
+    ms = min(ref.eclref_apsp_gpu(g.nodes, g.edges, Q(g.nindex), Q(g.nlist), Q(g.eweight), Q(out)) for _ in range(2))
+    return {"value": float(g.nodes) ** 3 / (ms / 1e3), "unit": "updates/s", "per_code": {"apsp": {"ms": ms}},
+            "note": "reference FW_gpu_64 (nvcc -O3 sm_100a), same graph, its printed compute time"}
+
+
 def reference_gpu(ecl, sym, dirg):
     """The reference's race-free CUDA build (oracle/_ref) on the same graphs:
     kernel time as each reference driver times it."""
@@ -649,10 +761,59 @@ def reference_gpu(ecl, sym, dirg):
             "note": "reference race-free CUDA build (nvcc -O3 sm_100a), same graphs, its own timed regions"}
 
 
+def run_reference_small(args, ecl):
+    """Reference arm of the grid and APSP workloads."""
+    orc, ref = _orc(), _ref()
+    if args.workload == "grid":
+        g = grid_graph(ecl)
+        for _ in range(min(args.warmup, 1)):
+            cpu_grid_once(g, orc)
+        u, t = 0.0, 0.0
+        for _ in range(args.steps):
+            du, dt = cpu_grid_once(g, orc)
+            u, t = u + du, t + dt
+        kind, unit = "port", "edges/s"
+        sample = "the full 1024x1024 grid, serial C oracle CC (the reference has no CPU CC solver)"
+        wl = f"grid1024-cc (n={g.nodes}, m={g.edges})"
+        metric = "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)"
+        try:
+            gpu = reference_gpu_grid(g)
+        except Exception as ex:
+            gpu = {"error": str(ex)}
+    else:
+        g = apsp_graph(ecl, APSP_CPU_N)
+        u, t, kind = 0.0, 0.0, "port"
+        for _ in range(args.steps):  # no warm-up: each closure takes seconds
+            du, dt, kind = cpu_apsp_once(g, orc, ref)
+            u, t = u + du, t + dt
+        unit = "updates/s"
+        sample = f"serial closure on ER n={APSP_CPU_N} ({'reference FW_cpu' if kind == 'reference' else 'C oracle'})"
+        wl = "er8192-apsp (CPU sample: n=%d)" % APSP_CPU_N
+        metric = "updates/s (n^3 / compute time of the blocked Floyd-Warshall closure; inputs resident)"
+        try:
+            gpu = reference_gpu_apsp(apsp_graph(ecl))
+        except Exception as ex:
+            gpu = {"error": str(ex)}
+    value = u / t
+    line = {
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators)",
+        "config": {"workload": wl, "parallelism": "host cores"},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": 1, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
     import ecl_b200 as ecl
+
+    if args.workload in ("grid", "apsp"):
+        return run_reference_small(args, ecl)
 
     orc = _orc()
     ref = _ref()

@@ -83,14 +83,41 @@ __device__ __forceinline__ int cc_link(int a, int b, int* parent) {
     }
     const int seen = cas(&parent[a], a, b);
     if (seen == a) return b;
+    // Another thread already hung a under b: the two trees are one.  On a
+    // mesh every vertex of a column links the same pair of roots, and all but
+    // one would otherwise walk the freshly linked chain of roots.
+    if (seen == b) return b;
     a = cc_root(seen, parent);
     b = cc_root(b, parent);
   }
   return a;
 }
 
+// Joins the trees of u and v without first walking to either root (the Link
+// step of Sutton, Ben-Nun and Barak, IPDPS 2018): look one level above the
+// larger side; if that already is the smaller side the trees are one, if it
+// is a root hang it under the smaller side, otherwise climb two levels and
+// retry.  Parents only point at smaller ids, so the loop ends.  A mesh links
+// the same pair of roots from every vertex of a column; a full root walk
+// there follows a chain of roots that grows while it is being walked.
+__device__ __forceinline__ void cc_union(int u, int v, int* parent) {
+  int p1 = ld(&parent[u]);
+  int p2 = ld(&parent[v]);
+  while (p1 != p2) {
+    const int high = max(p1, p2), low = min(p1, p2);
+    const int ph = ld(&parent[high]);
+    if (ph == low) return;
+    if (ph == high && cas(&parent[high], high, low) == high) return;
+    p1 = ld(&parent[ld(&parent[high])]);
+    p2 = ld(&parent[low]);
+  }
+}
+
 // Also checks the CSR rows once: a malformed row (end < beg, or outside
 // [0, m]) raises ECL_ERR_BAD_GRAPH and is treated as empty by every kernel.
+// kHook = false: every vertex starts as its own root (the symmetric path,
+// whose sampling rounds do the first links).
+template <bool kHook>
 __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ parent,
                                                 Status* __restrict__ status) {
@@ -104,7 +131,7 @@ __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restr
     // start (the labels do not depend on it), and scanning a whole hub row
     // from one thread would serialise a 163k-entry R-MAT hub.
     int p = v;
-    const int stop = min(end, beg + kInitScan);
+    const int stop = kHook ? min(end, beg + kInitScan) : beg;
     for (int i = beg; i < stop; i++) {
       const int u = __ldg(&nlist[i]);
       if (u < v && u >= 0) {
@@ -188,13 +215,22 @@ __global__ void __launch_bounds__(kTPB) cc_chunks(int n, const int* __restrict__
   }
 }
 
+// parent[v] = root(v) by pointer jumping: each thread only rewrites its own
+// parent[v], once per step, and steps to the parent of its current target.
+// Threads on the same chain run side by side, so every step reads a target
+// that has itself jumped -- a chain of depth D is flattened in about log2(D)
+// dependent loads per thread instead of D (a mesh builds chains as long as a
+// grid column).  parent[v] has no other writer during the launch, so the
+// array ends fully flat.
 __global__ void __launch_bounds__(kTPB) cc_flatten(int n, int* __restrict__ parent) {
   for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
-    int cur = ld(&parent[v]);
-    const int first = cur;
-    int next;
-    while (cur > (next = ld(&parent[cur]))) cur = next;
-    if (cur != first) st(&parent[v], cur);
+    int p = ld(&parent[v]);
+    if (p == v) continue;
+    int pp;
+    while ((pp = ld(&parent[p])) < p) {
+      st(&parent[v], pp);
+      p = pp;
+    }
   }
 }
 
@@ -208,21 +244,20 @@ __global__ void __launch_bounds__(kTPB) cc_flatten(int n, int* __restrict__ pare
 
 constexpr int kSample = 2;  // list entries linked per vertex before the skip
 
+// Sampling round r: links v with the r-th entry of its list.  The rounds run
+// as separate launches with a full compression in between, so every find of
+// the next round starts one step from its root -- on a mesh, linking both
+// samples at once builds chains as long as a grid column.
 __global__ void __launch_bounds__(kTPB) cc_sample(int n, int m, const int* __restrict__ nindex,
-                                                  const int* __restrict__ nlist, int* __restrict__ parent,
+                                                  const int* __restrict__ nlist, int* __restrict__ parent, int r,
                                                   Status* __restrict__ status) {
   for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
     int beg, end;
     cc_row(nindex, v, m, beg, end);
-    const int stop = min(end, beg + kSample);
-    int rv = -1;
-    for (int i = beg; i < stop; i++) {
-      const int u = __ldg(&nlist[i]);
-      if (u == v || !cc_valid(u, n, status)) continue;
-      if (rv < 0) rv = cc_root(v, parent);
-      const int ru = cc_root(u, parent);
-      if (ru != rv) rv = cc_link(rv, ru, parent);
-    }
+    if (beg + r >= end) continue;
+    const int u = __ldg(&nlist[beg + r]);
+    if (u == v || !cc_valid(u, n, status)) continue;
+    cc_union(v, u, parent);
   }
 }
 
@@ -379,9 +414,11 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   const int grid = dev.grid_blocks(kTPB);
   ECL_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(CCCounters), stream));
   if (g.flags & ECL_GRAPH_SYMMETRIC) {
-    ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
-    ECL_LAUNCH(cc_sample, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
-    ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
+    ECL_LAUNCH(cc_init<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
+    for (int r = 0; r < kSample; r++) {
+      ECL_LAUNCH(cc_sample, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, r, status);
+      ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
+    }
     ECL_LAUNCH(cc_giant, 1, 1024, 0, stream, g.n, parent, ctr);
     ECL_LAUNCH(cc_mark_giant, grid, kTPB, 0, stream, g.n, parent, ctr, ing);
     mark();
@@ -393,7 +430,7 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
     mark();
     return ECL_OK;
   }
-  ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
+  ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
   mark();
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, ctr, status);
   mark();
@@ -494,7 +531,7 @@ extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t
   // the counters (adjacent, at the front of the array) before every solve.
   ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
   const int grid = dev.grid_blocks(kTPB);
-  ECL_LAUNCH(cc_init, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
+  ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, ctr, status);
   ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, ctr, status);
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, nodes, label);

@@ -100,6 +100,7 @@ _sig("ecl_status_string", C.c_char_p, [C.c_int])
 _sig("ecl_last_error", C.c_char_p, [])
 _sig("ecl_workspace_bytes", C.c_size_t, [C.c_int, _I32, _I32])
 _sig("ecl_kernel_launches", C.c_uint64, [])
+_sig("ecl_minplus_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double)])
 _sig("ecl_cc", C.c_int, [_PV, _VP, _PO])
 _sig("ecl_mis", C.c_int, [_PV, _VP, _PO])
 _sig("ecl_gc", C.c_int, [_PV, _VP, _PO])
@@ -117,6 +118,7 @@ _sig("ecl_gen_er", C.c_int, [_I32, _F64, _U64, _I32, _U64, _I32, _I32, _PG])
 # Every symbol that include/ecl_b200.h declares (checked by the CPU tests).
 EXPORTED = [
     "ecl_abi_version", "ecl_status_string", "ecl_last_error", "ecl_workspace_bytes", "ecl_kernel_launches",
+    "ecl_minplus_peak",
     "ecl_cc", "ecl_mis", "ecl_gc", "ecl_mst", "ecl_scc", "ecl_apsp",
     "ecl_compute_cc", "ecl_compute_mis", "ecl_compute_gc", "ecl_compute_mst", "ecl_compute_scc", "ecl_compute_apsp",
     "ecl_graph_read", "ecl_graph_write", "ecl_graph_free", "ecl_graph_validate",
@@ -364,6 +366,14 @@ def _torch_dtype(name):
 
 def kernel_launches() -> int:
     return int(lib.ecl_kernel_launches())
+
+
+def minplus_peak(variant: int = 0) -> float:
+    """Measured INT32 min-plus rate of the current device, integer ops/s
+    (variant 0: DPX add-min, the APSP instruction; 1: separate add and min)."""
+    v = C.c_double(0.0)
+    _check(lib.ecl_minplus_peak(variant, C.byref(v)), "ecl_minplus_peak")
+    return float(v.value)
 
 
 # ---- batched engine (include/ecl_batch.h) ------------------------------------------

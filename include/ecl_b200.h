@@ -100,6 +100,12 @@ const char* ecl_last_error(void);
 size_t ecl_workspace_bytes(ecl_code code, int32_t nodes, int32_t edges);
 /* Number of this library's kernel launches since load (a process-wide counter). */
 uint64_t ecl_kernel_launches(void);
+/* Measured INT32 min-plus throughput of the current device, in integer
+ * operations per second (one update = add + min = 2 operations): the roofline
+ * denominator of ecl_apsp.  variant 0 times the DPX add-min instruction the
+ * APSP kernels issue, variant 1 a separate add and min.  No counterpart in the
+ * reference. */
+ecl_status ecl_minplus_peak(int32_t variant, double* ops_per_s);
 
 /* ---- solvers ------------------------------------------------------------------ */
 
