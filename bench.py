@@ -399,6 +399,7 @@ def run_ours(args, rank, world, local_rank):
         return o
 
     per_code_ms = {c: 0.0 for c, _ in jobs}
+    per_code_rounds = {}
     phase_tot = {}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -414,6 +415,7 @@ def run_ours(args, rank, world, local_rank):
             ms = ev0.elapsed_time(ev1)
             if timed:
                 per_code_ms[code] += ms
+                per_code_rounds[code] = int(o.rounds)
                 for i in range(o.nphases):
                     key = (phase_code(code, g), i)
                     phase_tot[key] = phase_tot.get(key, 0.0) + o.phase_ms[i]
@@ -551,7 +553,8 @@ def run_ours(args, rank, world, local_rank):
             cpu = cpu_baseline_apsp(ecl)
 
     per_code = {c: {"edges": g.edges, "ms": per_code_ms[c] / args.steps,
-                    "edges_per_s": g.edges / (per_code_ms[c] / args.steps / 1e3)} for c, g in jobs}
+                    "edges_per_s": g.edges / (per_code_ms[c] / args.steps / 1e3),
+                    "rounds": per_code_rounds.get(c)} for c, g in jobs}
     phases = {f"{PHASE_NAMES[c][i]}": round(v / args.steps, 4) for (c, i), v in sorted(phase_tot.items())}
     metric = ("updates/s (n^3 / compute time of the blocked Floyd-Warshall closure; inputs resident)" if is_apsp else
               "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)")

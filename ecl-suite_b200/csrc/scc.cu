@@ -11,16 +11,23 @@
 //
 // B200 design:
 //  * scc_mark / scc_build trim first: a vertex with no in-entry or no
-//    out-entry (self-loops ignored) is its own SCC and contributes no edge;
-//    only edges between two untrimmed vertices enter the int2 worklist
-//    (warp-aggregated appends).  Both passes are degree-binned (lane / warp /
-//    256-entry chunk records), so hub rows spread over all warps;
+//    out-entry (self-loops ignored) is its own SCC and contributes no edge.
+//    scc_build writes the int2 edge list in CSR positions -- slot i holds
+//    (v, nlist[i]) when both ends are live, else a dead slot -- so it is one
+//    streaming pass with no shared append counter (on R-MAT nearly every
+//    edge survives the trim, so compacting it would buy nothing).  Both
+//    passes are degree-binned (lane / warp / 256-entry chunk records), so
+//    hub rows spread over all warps;
 //  * scc_solve runs EVERY propagation sweep and every trimming round in one
 //    cooperative persistent launch, separated by bounded grid barriers (the
-//    reference pays a host round trip per propagation launch, :283-287);
-//    in-max / out-max live in two int arrays updated with fetch_max, and each
-//    sweep jumps through imax[imax[v]] / omax[omax[w]] (both still valid
-//    bounds) so values travel many hops per sweep;
+//    reference pays a host round trip per propagation launch, :283-287).
+//    In-max and out-max of a vertex share one 64-bit word (in-max high, out-
+//    max low), like the reference's iomax, so an edge costs two word loads
+//    plus two for the jumps io[in-max(v)] / io[out-max(w)] (both still valid
+//    bounds, so values travel many hops per sweep); a raise is a 32-bit
+//    atomic max on one half;
+//  * rounds after the first compact the surviving edges (the edges whose two
+//    ends share both values and are unresolved: io[v] == io[w]);
 //  * the final labels are written by the same launch (label = in-max).
 #include "csr_bins.cuh"
 #include "grid_sync.cuh"
@@ -36,9 +43,7 @@ constexpr int kMaxSweeps = 1 << 16;
 
 struct SCCCtl {
   GridBarrier bar;
-  int nedges;       // initial worklist size
-  int sizes[2];     // unused slot for alignment
-  int pad[61];
+  int pad[64];
   int changed[kMaxSweeps];   // per-sweep "something moved" flags
 };
 
@@ -47,25 +52,47 @@ struct SCCRound {
   int again;
 };
 
+// In-max (high half) and out-max (low half) of one vertex.
+__device__ __forceinline__ unsigned long long io_pack(int in, int out) {
+  return ((unsigned long long)(unsigned)in << 32) | (unsigned)out;
+}
+__device__ __forceinline__ int io_in(unsigned long long x) { return (int)(x >> 32); }
+__device__ __forceinline__ int io_out(unsigned long long x) { return (int)(unsigned)x; }
+
+// Raises the in-max (kIn) or out-max half of *p to val when `old`, the word
+// last read, is below it; true when it was.  The raise is a 32-bit atomic max
+// on that half: a word is read whole and raised per half, the reference's own
+// access pattern (readFirst / writeFirstA on iomax, ECL-SCC_10-atomic.cu:145-
+// 160), and a max never lowers a value another thread raised meanwhile.
+template <bool kIn>
+__device__ __forceinline__ bool io_raise(unsigned long long* p, unsigned long long old, int val) {
+  if ((kIn ? io_in(old) : io_out(old)) >= val) return false;
+  fetch_max(reinterpret_cast<int*>(p) + (kIn ? 1 : 0), val);  // little-endian: high half at +1
+  return true;
+}
+
 // A vertex is live (can be in a non-trivial SCC) iff it has an in-entry and an
-// out-entry other than self-loops.  scc_mark sets hasin[w] for every entry
-// w != v (plain relaxed stores of 1: idempotent) and hasout[v] for every v
+// out-entry other than self-loops.  Both facts share one flag word per vertex
+// (kHasIn | kHasOut), so the liveness test is one load; scc_mark ORs kHasIn
+// into flags[w] for every entry w != v and kHasOut into flags[v] for every v
 // with such an entry; rows longer than kBinChunk go to chunk records.
-__device__ __forceinline__ void scc_mark_entry(bool valid, int v, int w, int n, int* hasin, bool& out,
+constexpr int kHasIn = 1, kHasOut = 2;
+
+__device__ __forceinline__ void scc_mark_entry(bool valid, int v, int w, int n, int* flags, bool& out,
                                                Status* status) {
   if (!valid) return;
   if ((unsigned)w >= (unsigned)n) {
     raise(status, ECL_ERR_BAD_GRAPH, w);
   } else if (w != v) {
-    st(&hasin[w], 1);
+    fetch_or(&flags[w], kHasIn);
     out = true;
   }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __restrict__ nindex,
-                                                 const int* __restrict__ nlist, int* __restrict__ hasin,
-                                                 int* __restrict__ hasout, int* __restrict__ imax,
-                                                 int* __restrict__ omax, RowChunks rc, Status* __restrict__ status) {
+                                                 const int* __restrict__ nlist, int* __restrict__ flags,
+                                                 unsigned long long* __restrict__ io,
+                                                 RowChunks rc, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -74,8 +101,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     int beg = 0, end = 0;
     if (v < n) {
       csr_row(nindex, v, m, beg, end, status);
-      imax[v] = v;
-      omax[v] = v;
+      io[v] = io_pack(v, v);
     }
     const int deg = end - beg;
     if (deg > kBinChunk) push_row_chunks(rc, v, beg, end);
@@ -84,7 +110,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k = 0; k < kmax; k++) {
       const bool valid = lanelvl && k < deg;
-      scc_mark_entry(valid, v, valid ? __ldg(&nlist[beg + k]) : 0, n, hasin, out, status);
+      scc_mark_entry(valid, v, valid ? __ldg(&nlist[beg + k]) : 0, n, flags, out, status);
     }
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
@@ -94,16 +120,16 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       bool wout = false;
-      for (int i = wbeg + lane; i < wend; i += 32) scc_mark_entry(true, wv, __ldg(&nlist[i]), n, hasin, wout, status);
+      for (int i = wbeg + lane; i < wend; i += 32) scc_mark_entry(true, wv, __ldg(&nlist[i]), n, flags, wout, status);
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
-    if (v < n) hasout[v] = (deg <= kBinChunk && out) ? 1 : 0;  // long rows: set by scc_mark_chunks
+    if (v < n && deg <= kBinChunk && out) fetch_or(&flags[v], kHasOut);  // long rows: scc_mark_chunks
   }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
-                                                        const int* __restrict__ nlist, int* __restrict__ hasin,
-                                                        int* __restrict__ hasout, RowChunks rc,
+                                                        const int* __restrict__ nlist, int* __restrict__ flags,
+                                                        RowChunks rc,
                                                         Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -113,42 +139,41 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     const int2 r = rc.rec[c];
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
-    for (int i = r.y + lane; i < end; i += 32) scc_mark_entry(true, r.x, __ldg(&nlist[i]), n, hasin, out, status);
-    if (__any_sync(kFull, out) && lane == 0) st(&hasout[r.x], 1);
+    for (int i = r.y + lane; i < end; i += 32) scc_mark_entry(true, r.x, __ldg(&nlist[i]), n, flags, out, status);
+    if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
   }
 }
 
-__device__ __forceinline__ bool scc_live(const int* hasin, const int* hasout, int v) {
-  return ld(&hasin[v]) != 0 && ld(&hasout[v]) != 0;
+__device__ __forceinline__ bool scc_live(const int* flags, int v) {
+  return ld(&flags[v]) == (kHasIn | kHasOut);
+}
+
+__device__ __forceinline__ int2 scc_slot(bool live_v, int v, int w, int n, const int* flags) {
+  const bool keep = live_v && w != v && (unsigned)w < (unsigned)n && scc_live(flags, w);
+  return keep ? make_int2(v, w) : make_int2(-1, -1);
 }
 
 __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __restrict__ nindex,
-                                                  const int* __restrict__ nlist, const int* __restrict__ hasin,
-                                                  const int* __restrict__ hasout, int2* __restrict__ wl,
-                                                  SCCCtl* __restrict__ ctl) {
+                                                  const int* __restrict__ nlist, const int* __restrict__ flags,
+                                                  int2* __restrict__ wl) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   for (int base = warp * 32; base < n; base += nwarps * 32) {
     const int v = base + lane;
     int beg = 0, end = 0;
-    if (v < n && scc_live(hasin, hasout, v)) {
+    bool live = false;
+    if (v < n) {
       beg = __ldg(&nindex[v]);
       end = __ldg(&nindex[v + 1]);
-      if (beg < 0 || end < beg || end > m) beg = end = 0;
+      if (beg < 0 || end < beg || end > m) beg = end = 0;  // reported by scc_mark
+      live = scc_live(flags, v);
     }
     const int deg = end - beg;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k = 0; k < kmax; k++) {
-      bool keep = false;
-      int w = 0;
-      if (lanelvl && k < deg) {
-        w = __ldg(&nlist[beg + k]);
-        keep = w != v && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
-      }
-      const int at = warp_append(&ctl->nedges, keep);
-      if (keep) wl[at] = make_int2(v, w);
+      if (lanelvl && k < deg) wl[beg + k] = scc_slot(live, v, __ldg(&nlist[beg + k]), n, flags);
     }
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
@@ -157,54 +182,38 @@ __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __res
       const int wv = __shfl_sync(kFull, v, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      for (int i0 = wbeg; i0 < wend; i0 += 32) {
-        bool keep = false;
-        int w = 0;
-        if (i0 + lane < wend) {
-          w = __ldg(&nlist[i0 + lane]);
-          keep = w != wv && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
-        }
-        const int at = warp_append(&ctl->nedges, keep);
-        if (keep) wl[at] = make_int2(wv, w);
-      }
+      const bool wlive = __shfl_sync(kFull, live, who);
+      for (int i = wbeg + lane; i < wend; i += 32) wl[i] = scc_slot(wlive, wv, __ldg(&nlist[i]), n, flags);
     }
   }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_build_chunks(int n, const int* __restrict__ nindex,
-                                                         const int* __restrict__ nlist, const int* __restrict__ hasin,
-                                                         const int* __restrict__ hasout, int2* __restrict__ wl,
-                                                         SCCCtl* __restrict__ ctl, RowChunks rc) {
+                                                         const int* __restrict__ nlist, const int* __restrict__ flags,
+                                                         int2* __restrict__ wl,
+                                                         RowChunks rc) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   const int total = *rc.count;
   for (int c = warp; c < total; c += nwarps) {
     const int2 r = rc.rec[c];
-    if (!scc_live(hasin, hasout, r.x)) continue;  // warp-uniform
+    const bool live = scc_live(flags, r.x);
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
-    for (int i0 = r.y; i0 < end; i0 += 32) {
-      bool keep = false;
-      int w = 0;
-      if (i0 + lane < end) {
-        w = __ldg(&nlist[i0 + lane]);
-        keep = w != r.x && (unsigned)w < (unsigned)n && scc_live(hasin, hasout, w);
-      }
-      const int at = warp_append(&ctl->nedges, keep);
-      if (keep) wl[at] = make_int2(r.x, w);
-    }
+    for (int i = r.y + lane; i < end; i += 32) wl[i] = scc_slot(live, r.x, __ldg(&nlist[i]), n, flags);
   }
 }
 
-__global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA, int2* __restrict__ wlB,
-                                                  int* __restrict__ imax, int* __restrict__ omax,
-                                                  int* __restrict__ label, SCCCtl* __restrict__ ctl,
-                                                  SCCRound* __restrict__ rounds, int max_rounds,
-                                                  Status* __restrict__ status) {
+// Round 0 sweeps the CSR-position edge list of `m0` slots (dead slots have
+// x < 0); later rounds sweep the compacted survivors.
+__global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
+                                                  unsigned long long* __restrict__ io, int* __restrict__ label,
+                                                  SCCCtl* __restrict__ ctl, SCCRound* __restrict__ rounds,
+                                                  int max_rounds, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int tid = blockIdx.x * kTPB + threadIdx.x;
   const int nthreads = gridDim.x * kTPB;
-  int size = ld(&ctl->nedges);
+  int size = m0;
   int sweep = 0;
   int round = 0;
   int2* cur = wlA;
@@ -221,21 +230,28 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA,
         return;
       }
       bool moved = false;
-      for (int i = tid; i < size; i += nthreads) {
-        const int2 e = cur[i];
+      // Whole warps step together: in CSR order neighbouring lanes mostly
+      // share v, so the out-max raises of v are combined per warp
+      // (__match_any_sync + max) into one atomic instead of up to 32 on one
+      // address.
+      for (int i0 = tid - lane; i0 < size; i0 += nthreads) {
+        const int i = i0 + lane;
+        const int2 e = i < size ? cur[i] : make_int2(-1, -1);
         const int v = e.x, w = e.y;
-        int iv = ld(&imax[v]);
-        if (iv != v) iv = max(iv, ld(&imax[iv]));
-        if (ld(&imax[w]) < iv) {
-          fetch_max(&imax[w], iv);
-          moved = true;
+        unsigned long long A = 0;
+        int ow = -1;
+        if (v >= 0) {
+          A = ld(&io[v]);
+          const unsigned long long B = ld(&io[w]);
+          int iv = io_in(A);
+          if (iv != v) iv = max(iv, io_in(ld(&io[iv])));
+          ow = io_out(B);
+          if (ow != w) ow = max(ow, io_out(ld(&io[ow])));
+          if (io_raise<true>(&io[w], B, iv)) moved = true;
         }
-        int ow = ld(&omax[w]);
-        if (ow != w) ow = max(ow, ld(&omax[ow]));
-        if (ld(&omax[v]) < ow) {
-          fetch_max(&omax[v], ow);
-          moved = true;
-        }
+        const unsigned grp = __match_any_sync(kFull, v);
+        const int gow = __reduce_max_sync(grp, ow);
+        if (v >= 0 && lane == __ffs(grp) - 1 && io_raise<false>(&io[v], A, gow)) moved = true;
       }
       if (__any_sync(kFull, moved) && lane == 0) st(&ctl->changed[sweep], 1);
       if (!grid_sync(&ctl->bar, status)) return;
@@ -250,8 +266,10 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA,
       int2 e = make_int2(0, 0);
       if (i < size) {
         e = cur[i];
-        const int iv = ld(&imax[e.x]), ov = ld(&omax[e.x]);
-        keep = iv != ov && iv == ld(&imax[e.y]) && ov == ld(&omax[e.y]);
+        if (e.x >= 0) {
+          const unsigned long long A = ld(&io[e.x]);
+          keep = io_in(A) != io_out(A) && A == ld(&io[e.y]);
+        }
       }
       const int at = warp_append(&rounds[round].size, keep);
       if (keep) nxt[at] = e;
@@ -260,12 +278,11 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA,
     // 3. retire resolved vertices, reset the rest to their own id
     bool again = false;
     for (int v = tid; v < n; v += nthreads) {
-      const int iv = ld(&imax[v]);
-      if (iv == ld(&omax[v])) {
-        label[v] = iv;
+      const unsigned long long A = ld(&io[v]);
+      if (io_in(A) == io_out(A)) {
+        label[v] = io_in(A);
       } else {
-        st(&imax[v], v);
-        st(&omax[v], v);
+        st(&io[v], io_pack(v, v));
         again = true;
       }
     }
@@ -283,12 +300,10 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int2* __restrict__ wlA,
 struct SCCBufs {
   SCCCtl* ctl;
   SCCRound* rounds;
-  int* hasin;
-  int* hasout;
+  int* flags;
   int* nchunks;
   int2* chunks;
-  int* imax;
-  int* omax;
+  unsigned long long* io;
   int2* wlA;
   int2* wlB;
   int max_rounds;
@@ -298,12 +313,10 @@ void scc_layout(Carve& c, int n, int m, SCCBufs* b) {
   b->ctl = c.take<SCCCtl>(1);
   b->max_rounds = n + 1;
   b->rounds = c.take<SCCRound>((size_t)b->max_rounds);
-  b->hasin = c.take<int>((size_t)n);
-  b->hasout = c.take<int>((size_t)n);
+  b->flags = c.take<int>((size_t)n);
   b->nchunks = c.take<int>(64);
   b->chunks = c.take<int2>(row_chunk_capacity(m));
-  b->imax = c.take<int>((size_t)n);
-  b->omax = c.take<int>((size_t)n);
+  b->io = c.take<unsigned long long>((size_t)n);
   b->wlA = c.take<int2>((size_t)(m > 0 ? m : 1));
   b->wlB = c.take<int2>((size_t)(m > 0 ? m : 1));
 }
@@ -336,17 +349,16 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaMemsetAsync(b.ctl, 0, sizeof(SCCCtl), stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.rounds, 0, sizeof(SCCRound) * (size_t)b.max_rounds, stream) != cudaSuccess)
     return ECL_ERR_CUDA;
-  if (cudaMemsetAsync(b.hasin, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
+  if (cudaMemsetAsync(b.flags, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks};
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.hasin, b.hasout, b.imax, b.omax, rc,
-             status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.hasin, b.hasout, rc, status);
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.io, rc, status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, rc, status);
   mark();
-  ECL_LAUNCH(scc_build, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.hasin, b.hasout, b.wlA, b.ctl);
-  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.hasin, b.hasout, b.wlA, b.ctl, rc);
+  ECL_LAUNCH(scc_build, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA);
+  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc);
   mark();
-  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, b.wlA, b.wlB, b.imax, b.omax, label, b.ctl,
+  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.io, label, b.ctl,
                                   b.rounds, max_rounds, status));
   mark();
   return ECL_OK;
