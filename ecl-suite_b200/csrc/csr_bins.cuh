@@ -53,5 +53,45 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
   return pred ? base + __popc(bal & ((1u << lane) - 1)) : -1;
 }
 
+// Per-warp staging of an append-only list in shared memory.  Lanes append
+// into the warp's own kCap-slot buffer (ballot + popc, no atomics); when fewer
+// than 32 slots are left the warp reserves room in the global list with ONE
+// atomic and writes the buffer out with coalesced stores.  A global counter
+// then sees one atomic per ~kCap entries instead of one per warp step --
+// appends from every warp of the grid to a single counter serialise in L2.
+// All lanes call push() and flush() together; flush() once more at the end.
+template <typename T, int kCap>
+struct WarpStage {
+  T* buf;         // this warp's kCap slots in shared memory
+  int count = 0;  // warp-uniform
+
+  // `overflow` is set when the global list (capacity `cap`) is full; the
+  // entries that did not fit are dropped.
+  __device__ __forceinline__ void push(bool pred, const T& item, T* out, int* counter, long long cap, bool& overflow) {
+    const int lane = threadIdx.x & 31;
+    const unsigned bal = __ballot_sync(kFull, pred);
+    if (pred) buf[count + __popc(bal & ((1u << lane) - 1))] = item;
+    count += __popc(bal);
+    if (count > kCap - 32) flush(out, counter, cap, overflow);
+  }
+
+  __device__ __forceinline__ void flush(T* out, int* counter, long long cap, bool& overflow) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (count == 0) return;
+    int base = 0;
+    if (lane == 0) base = fetch_add(counter, count);
+    base = __shfl_sync(kFull, base, 0);
+    for (int i = lane; i < count; i += 32) {
+      if ((long long)base + i < cap)
+        out[base + i] = buf[i];
+      else
+        overflow = true;
+    }
+    __syncwarp();
+    count = 0;
+  }
+};
+
 }  // namespace dev
 }  // namespace ecl

@@ -13,7 +13,8 @@
 //    the quantile that leaves ~1.5 n light edges (no host round trip);
 //  * mst_scan: builds a worklist of int4 {a, b, weight, j} from the CSR,
 //    lane-level for lists <= 32 entries, warp-level up to kChunk, chunk
-//    records beyond; appends are warp-aggregated (one atomic per warp step);
+//    records beyond; appends are staged per warp in shared memory and
+//    reserved in the global list with one atomic per ~kStage entries;
 //    the heavy pass drops entries whose endpoints are already joined;
 //  * mst_boruvka: ALL Boruvka rounds in one cooperative persistent launch
 //    (2 bounded grid barriers per round): phase A re-roots each edge, drops
@@ -24,6 +25,7 @@
 //    no counter is ever reset concurrently with its use.
 #include <cooperative_groups.h>
 
+#include "csr_bins.cuh"
 #include "grid_sync.cuh"
 #include "solvers.cuh"
 
@@ -73,17 +75,6 @@ __device__ __forceinline__ void mst_join(int a, int b, int* parent) {
     }
     if (cas(&parent[a], a, b) == a) return;
   }
-}
-
-// Warp-aggregated append: every lane of `mask` must call this together.
-__device__ __forceinline__ int warp_slot(int* counter, bool pred, unsigned mask, int lane) {
-  const unsigned bal = __ballot_sync(mask, pred);
-  if (bal == 0) return -1;
-  const int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = fetch_add(counter, __popc(bal));
-  base = __shfl_sync(mask, base, leader);
-  return pred ? base + __popc(bal & ((1u << lane) - 1)) : -1;
 }
 
 __global__ void mst_init(int n, int* __restrict__ parent, u64* __restrict__ minv) {
@@ -137,42 +128,41 @@ __device__ __forceinline__ bool mst_keep(int w, int thr) {
   return kLight ? (w <= thr) : (w > thr);
 }
 
-// Emits the worklist entry for CSR entry j of vertex v (rv = v's root in the
-// heavy pass).  All lanes of `mask` call together.
+// Worklist entry for CSR entry j of vertex v (rv = v's root in the heavy
+// pass); returns whether it is kept.
 template <bool kLight>
-__device__ __forceinline__ void mst_emit(bool valid, int v, int rv, int j, int n, const int* nlist, const int* eweight,
-                                         int thr, int* parent, int4* wl, int* cnt, int cap, unsigned mask, int lane,
-                                         Status* status) {
-  bool keep = false;
-  int4 e;
-  if (valid) {
-    const int u = __ldg(&nlist[j]);
-    if ((unsigned)u >= (unsigned)n) {
-      raise(status, ECL_ERR_BAD_GRAPH, u);
-    } else if (u > v) {
-      const int w = __ldg(&eweight[j]);
-      if (w < 0) {
-        raise(status, ECL_ERR_BAD_GRAPH, j);
-      } else if (mst_keep<kLight>(w, thr)) {
-        if (kLight) {
-          keep = true;
-          e = make_int4(v, u, w, j);
-        } else {
-          const int ru = mst_find(u, parent);
-          keep = ru != rv;
-          e = make_int4(rv, ru, w, j);
-        }
-      }
-    }
+__device__ __forceinline__ bool mst_entry(bool valid, int v, int rv, int j, int n, const int* nlist, const int* eweight,
+                                          int thr, int* parent, int4& e, Status* status) {
+  if (!valid) return false;
+  const int u = __ldg(&nlist[j]);
+  if ((unsigned)u >= (unsigned)n) {
+    raise(status, ECL_ERR_BAD_GRAPH, u);
+    return false;
   }
-  const int k = warp_slot(cnt, keep, mask, lane);
-  if (keep) {
-    if (k < cap) {
-      wl[k] = e;
-    } else {
-      raise(status, ECL_ERR_BAD_GRAPH, -2);  // more v<n entries than the capacity (asymmetric graph flagged symmetric)
-    }
+  if (u <= v) return false;
+  const int w = __ldg(&eweight[j]);
+  if (w < 0) {
+    raise(status, ECL_ERR_BAD_GRAPH, j);
+    return false;
   }
+  if (!mst_keep<kLight>(w, thr)) return false;
+  if (kLight) {
+    e = make_int4(v, u, w, j);
+    return true;
+  }
+  const int ru = mst_find(u, parent);
+  e = make_int4(rv, ru, w, j);
+  return ru != rv;
+}
+
+// Slots per warp in the shared-memory staging of worklist appends.
+constexpr int kStage = 128;
+typedef WarpStage<int4, kStage> Stage;
+
+// More v<n entries than the worklist holds: an asymmetric graph flagged
+// symmetric.
+__device__ __forceinline__ void mst_overflow(bool overflow, Status* status) {
+  if (__any_sync(kFull, overflow) && (threadIdx.x & 31) == 0) raise(status, ECL_ERR_BAD_GRAPH, -2);
 }
 
 template <bool kLight>
@@ -186,6 +176,9 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
   const int nwarps = (gridDim.x * kTPB) >> 5;
   const int thr = ctl->threshold;
   int* cnt = &ctl->wlcount[kLight ? 0 : 1][0];
+  __shared__ int4 stage_buf[kTPB / 32][kStage];
+  Stage stg{stage_buf[threadIdx.x >> 5]};
+  bool overflow = false;
   for (int base = warp * 32; base < n; base += nwarps * 32) {
     const int v = base + lane;
     int beg = 0, end = 0;
@@ -209,8 +202,10 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
     // lane level: all lanes step through offset k together
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k = 0; k < kmax; k++) {
-      const bool valid = lanelvl && k < deg;
-      mst_emit<kLight>(valid, v, rv, beg + k, n, nlist, eweight, thr, parent, wl, cnt, cap, kFull, lane, status);
+      int4 e;
+      const bool keep = mst_entry<kLight>(lanelvl && k < deg, v, rv, beg + k, n, nlist, eweight, thr, parent, e,
+                                          status);
+      stg.push(keep, e, wl, cnt, cap, overflow);
     }
     // warp level
     unsigned todo = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
@@ -222,11 +217,15 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       for (int i0 = wbeg; i0 < wend; i0 += 32) {
-        mst_emit<kLight>(i0 + lane < wend, wv, wrv, i0 + lane, n, nlist, eweight, thr, parent, wl, cnt, cap, kFull,
-                         lane, status);
+        int4 e;
+        const bool keep = mst_entry<kLight>(i0 + lane < wend, wv, wrv, i0 + lane, n, nlist, eweight, thr, parent, e,
+                                            status);
+        stg.push(keep, e, wl, cnt, cap, overflow);
       }
     }
   }
+  stg.flush(wl, cnt, cap, overflow);
+  mst_overflow(overflow, status);
   // chunk records (hubs): the light pass sees them only after all warps
   // passed the vertex loop, so they are handled by mst_chunks.
 }
@@ -242,27 +241,37 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
   const int thr = ctl->threshold;
   int* cnt = &ctl->wlcount[kLight ? 0 : 1][0];
   const int total = ctl->nchunks;
+  __shared__ int4 stage_buf[kTPB / 32][kStage];
+  Stage stg{stage_buf[threadIdx.x >> 5]};
+  bool overflow = false;
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
     const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
     const int rv = kLight ? v : mst_find(v, parent);
     for (int i0 = rec.y; i0 < end; i0 += 32) {
-      mst_emit<kLight>(i0 + lane < end, v, rv, i0 + lane, n, nlist, eweight, thr, parent, wl, cnt, cap, kFull, lane,
-                       status);
+      int4 e;
+      const bool keep = mst_entry<kLight>(i0 + lane < end, v, rv, i0 + lane, n, nlist, eweight, thr, parent, e,
+                                          status);
+      stg.push(keep, e, wl, cnt, cap, overflow);
     }
   }
+  stg.flush(wl, cnt, cap, overflow);
+  mst_overflow(overflow, status);
 }
 
 // All Boruvka rounds of one pass.  wlA holds the pass's initial worklist
 // (size wlcount[pass][0]); rounds alternate wlA/wlB.
 __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __restrict__ wlA, int4* __restrict__ wlB,
-                                                    int* __restrict__ parent, u64* __restrict__ minv,
+                                                    int cap, int* __restrict__ parent, u64* __restrict__ minv,
                                                     unsigned char* __restrict__ in_mst, MSTCtl* __restrict__ ctl,
                                                     Status* __restrict__ status) {
   const int tid = blockIdx.x * kTPB + threadIdx.x;
   const int nthreads = gridDim.x * kTPB;
   int* cnt = ctl->wlcount[pass];
+  __shared__ int4 stage_buf[kTPB / 32][kStage];
+  Stage stg{stage_buf[threadIdx.x >> 5]};
+  bool overflow = false;
   u64 local = 0;
   int r = 0;
   for (; r < kMaxRounds; r++) {
@@ -270,7 +279,9 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     int4* out = (r & 1) ? wlA : wlB;
     u64* mcur = minv + (size_t)(r & 1) * n;
     u64* mprev = minv + (size_t)((r + 1) & 1) * n;
-    const int sz = ld(&cnt[r]);
+    // a scan that overflowed (reported as BAD_GRAPH) counted more entries
+    // than the list holds
+    const int sz = min(ld(&cnt[r]), cap);
     // phase A: re-root, drop intra-component edges, publish keys.  The trip
     // count is uniform across the grid so every warp step is converged for
     // the warp-aggregated append.
@@ -290,16 +301,14 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
         rb = mst_find(e.y, parent);
         keep = ra != rb;
       }
-      const int k = warp_slot(&cnt[r + 1], keep, kFull, threadIdx.x & 31);
+      stg.push(keep, make_int4(ra, rb, e.z, e.w), out, &cnt[r + 1], cap, overflow);
       if (keep) {
-        e.x = ra;
-        e.y = rb;
-        out[k] = e;
         const u64 key = ((u64)(unsigned)e.z << 32) | (unsigned)e.w;
         if (ld(&mcur[ra]) > key) fetch_min(&mcur[ra], key);
         if (ld(&mcur[rb]) > key) fetch_min(&mcur[rb], key);
       }
     }
+    stg.flush(out, &cnt[r + 1], cap, overflow);
     if (!grid_sync(&ctl->bar, status)) return;
     const int nsz = ld(&cnt[r + 1]);
     if (nsz == 0) break;
@@ -384,8 +393,8 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
                    b.ctl, b.chunks, status);
       }
       mark();
-      ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.parent, b.minv,
-                                      in_mst, b.ctl, status));
+      ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.cap, b.parent,
+                                      b.minv, in_mst, b.ctl, status));
       mark();
       // The heavy pass (pass 1) runs unconditionally: with no filter it finds
       // no entry above the INT_MAX threshold and ends after one round.
