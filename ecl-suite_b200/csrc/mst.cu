@@ -15,7 +15,8 @@
 //    lane-level for lists <= 32 entries, warp-level up to kChunk, chunk
 //    records beyond; appends are staged per warp in shared memory and
 //    reserved in the global list with one atomic per ~kStage entries;
-//    the heavy pass drops entries whose endpoints are already joined;
+//    the heavy pass drops entries whose endpoints are already joined (the
+//    forest is flattened by pointer jumping first, so a root is one load);
 //  * mst_boruvka: ALL Boruvka rounds in one cooperative persistent launch
 //    (2 bounded grid barriers per round): phase A re-roots each edge, drops
 //    intra-component edges and atomicMin's its key into both roots; phase B
@@ -74,6 +75,22 @@ __device__ __forceinline__ void mst_join(int a, int b, int* parent) {
       b = t;
     }
     if (cas(&parent[a], a, b) == a) return;
+  }
+}
+
+// parent[v] = root(v) between the passes, so the heavy scan reads each
+// entry's root with one load.  Pointer jumping: each thread rewrites only its
+// own parent[v] (parents point at smaller ids), stepping to the parent of its
+// current target, which its own thread is shortening at the same time.
+__global__ void __launch_bounds__(kTPB) mst_flatten(int n, int* __restrict__ parent) {
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
+    int p = ld(&parent[v]);
+    if (p == v) continue;
+    int pp;
+    while ((pp = ld(&parent[p])) < p) {
+      st(&parent[v], pp);
+      p = pp;
+    }
   }
 }
 
@@ -150,7 +167,7 @@ __device__ __forceinline__ bool mst_entry(bool valid, int v, int rv, int j, int 
     e = make_int4(v, u, w, j);
     return true;
   }
-  const int ru = mst_find(u, parent);
+  const int ru = ld(&parent[u]);  // flat after mst_flatten
   e = make_int4(rv, ru, w, j);
   return ru != rv;
 }
@@ -193,7 +210,7 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
     const int deg = end - beg;
     const bool lanelvl = deg > 0 && deg <= kLaneMax;
     int rv = v;
-    if (!kLight && deg > 0 && v < n) rv = mst_find(v, parent);
+    if (!kLight && deg > 0 && v < n) rv = ld(&parent[v]);
     if (kLight && deg > kChunk) {  // chunk records are built once, in the light pass
       const int nc = (deg + kChunk - 1) / kChunk;
       const int at = fetch_add(&ctl->nchunks, nc);
@@ -248,7 +265,7 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
     const int2 rec = chunks[c];
     const int v = rec.x;
     const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
-    const int rv = kLight ? v : mst_find(v, parent);
+    const int rv = kLight ? v : ld(&parent[v]);
     for (int i0 = rec.y; i0 < end; i0 += 32) {
       int4 e;
       const bool keep = mst_entry<kLight>(i0 + lane < end, v, rv, i0 + lane, n, nlist, eweight, thr, parent, e,
@@ -387,6 +404,7 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
         ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
                    b.ctl, b.chunks, status);
       } else {
+        ECL_LAUNCH(mst_flatten, grid, kTPB, 0, stream, g.n, b.parent);
         ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, status);
         ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
