@@ -27,9 +27,12 @@
 //    (about 2700 vertices at R-MAT-22, most of it in the hub core) costs one
 //    poll-and-store hop per vertex on it.
 //  * A long row is scanned by a whole warp with a 2048-colour bitmap in
-//    shared memory; claiming one long row per warp keeps every in-flight row
-//    of the dense hub core scanning concurrently, so a hop along the chain
-//    costs one poll, not a scan of the row.
+//    shared memory.  The first pass never blocks: colours already published
+//    go into the bitmap and the undecided entries into a per-warp pending
+//    list; lanes then wait on listed entries (one address per lane) and
+//    re-check the rest of the list without blocking -- so a hop along the
+//    chain costs one poll and a short re-check, not a rescan of the row
+//    (short rows: the same with a bit mask per lane).
 #include "csr_bins.cuh"
 #include "radix_sort.cuh"
 #include "solvers.cuh"
@@ -196,7 +199,9 @@ __device__ __forceinline__ unsigned long long gc_now() {
 }
 
 constexpr unsigned long long kStallNs = 2000000000ull;  // 2 s without progress -> give up
-constexpr int kMexWords = 64;                           // warp bitmap: 2048 colours per pass
+constexpr int kMexWords = 64;                           // warp bitmap: 2048 colours per window
+constexpr int kPend = 512;                              // per-warp list of undecided entries
+constexpr int kBatch = 8;                               // entries per lane whose loads are in flight together
 
 // Colour of u once it is published (bounded wait).  Returns -1 on a stall.
 __device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* status) {
@@ -215,18 +220,160 @@ __device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* s
   return c;
 }
 
+__device__ __forceinline__ void gc_mark(unsigned* bits, int c, int off) {
+  const int d = c - off;
+  if (d >= 0 && d < 32 * kMexWords) atomicOr(&bits[d >> 5], 1u << (d & 31));
+}
+
+// Colour of a long row: the smallest colour no entry of nl2[wb, we) uses.
+// Each window of 2048 colours starts with one non-blocking pass over the row:
+// colours already published go into the bitmap, still-undecided entries into
+// the per-warp list `pend`.  Then every lane waits (bounded, one address per
+// lane as before) for one listed entry, and the rest of the list is
+// re-checked without blocking and compacted; repeat until it is empty.  Once
+// the last dependency is coloured the row is one poll and one short re-check
+// from its colour -- a lane no longer walks the rest of its share of the row
+// after each wait.  The pass stops while the list still has room for a whole
+// step of 32 entries; the listed ones are resolved and the pass resumes where
+// it stopped, so every entry is read once by the pass.  Returns -1 on a
+// stall.  All lanes call.
+__device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend,
+                           Status* status) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1;
+  for (int off = 0;; off += 32 * kMexWords) {
+    bits[lane] = 0;
+    bits[lane + 32] = 0;
+    __syncwarp();
+    int cursor = wb;
+    while (cursor < we) {
+      int np = 0;
+      int i0 = cursor;
+      // kBatch entries per lane per step: all index loads, then all colour
+      // loads, are issued before any result is used (one round trip per
+      // 32 * kBatch entries instead of two per 32)
+      for (; i0 < we && np + 32 * kBatch <= kPend; i0 += 32 * kBatch) {
+        int u[kBatch], c[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+          const int i = i0 + 32 * k + lane;
+          u[k] = i < we ? __ldg(&nl2[i]) : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) c[k] = u[k] >= 0 ? ld(&color[u[k]]) : 0;
+#pragma unroll
+        for (int k = 0; k < kBatch; k++) {
+          const bool undecided = u[k] >= 0 && c[k] < 0;
+          if (u[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
+          const unsigned ub = __ballot_sync(kFull, undecided);
+          if (undecided) pend[np + __popc(ub & lt)] = u[k];
+          np += __popc(ub);
+        }
+      }
+      cursor = i0;  // the list is full or the row is done: resolve, then resume here
+      int cnt = np;
+      while (cnt > 0) {
+        __syncwarp();
+        bool stalled = false;
+        if (lane < cnt) {
+          const int c = gc_wait_colour(color, pend[lane], status);
+          if (c < 0)
+            stalled = true;
+          else
+            gc_mark(bits, c, off);
+        }
+        if (__any_sync(kFull, stalled)) return -1;
+        int kept = 0;
+        for (int j0 = 32; j0 < cnt; j0 += 32 * kBatch) {
+          int u[kBatch], c[kBatch];
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            const int j = j0 + 32 * k + lane;
+            u[k] = j < cnt ? pend[j] : -1;
+          }
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) c[k] = u[k] >= 0 ? ld(&color[u[k]]) : 0;
+          __syncwarp();  // every lane has read its slots before any is overwritten
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            const bool still = u[k] >= 0 && c[k] < 0;
+            if (u[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
+            const unsigned sb = __ballot_sync(kFull, still);
+            if (still) pend[kept + __popc(sb & lt)] = u[k];  // index < j0: already read
+            kept += __popc(sb);
+          }
+        }
+        cnt = kept;
+      }
+    }
+    __syncwarp();
+    const unsigned w0 = bits[lane], w1 = bits[lane + 32];
+    const unsigned f0 = __ballot_sync(kFull, w0 != ~0u), f1 = __ballot_sync(kFull, w1 != ~0u);
+    int c = -1;
+    if (f0) {
+      const int wi = __ffs(f0) - 1;
+      c = off + wi * 32 + __ffs(~__shfl_sync(kFull, w0, wi)) - 1;
+    } else if (f1) {
+      const int wi = __ffs(f1) - 1;
+      c = off + (wi + 32) * 32 + __ffs(~__shfl_sync(kFull, w1, wi)) - 1;
+    }
+    __syncwarp();
+    if (c >= 0) return c;
+  }
+}
+
+// Colour of a short row (h <= 32 entries at nl2[beg]): one lane, the same
+// scheme with a bit mask of the undecided entries -- wait for the first one,
+// re-check the others without blocking.  -1 on a stall.
+__device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, Status* status) {
+  unsigned long long used = 0;  // colour <= h <= 32
+  unsigned pendm = 0;
+  for (int k0 = 0; k0 < h; k0 += kBatch) {
+    int u[kBatch], c[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) u[k] = k0 + k < h ? __ldg(&nl2[beg + k0 + k]) : -1;
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) c[k] = u[k] >= 0 ? ld(&color[u[k]]) : 0;
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      if (u[k] < 0) continue;
+      if (c[k] >= 0)
+        used |= 1ull << (c[k] & 63);
+      else
+        pendm |= 1u << (k0 + k);
+    }
+  }
+  while (pendm) {
+    const int k0 = __ffs(pendm) - 1;
+    const int c0 = gc_wait_colour(color, __ldg(&nl2[beg + k0]), status);
+    if (c0 < 0) return -1;
+    used |= 1ull << (c0 & 63);
+    pendm &= pendm - 1;
+    for (unsigned mm = pendm; mm; mm &= mm - 1) {
+      const int k = __ffs(mm) - 1;
+      const int c = ld(&color[__ldg(&nl2[beg + k])]);
+      if (c >= 0) {
+        used |= 1ull << (c & 63);
+        pendm &= ~(1u << k);
+      }
+    }
+  }
+  return __ffsll((long long)~used) - 1;
+}
+
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
                                                 const int* __restrict__ hc, const int* __restrict__ order,
                                                 int* __restrict__ color, GCCtl* __restrict__ ctl,
                                                 Status* __restrict__ status) {
   __shared__ unsigned s_bits[kTPB / 32][kMexWords];
+  __shared__ int s_pend[kTPB / 32][kPend];
   const int lane = threadIdx.x & 31;
   unsigned* bits = s_bits[threadIdx.x >> 5];
+  int* pend = s_pend[threadIdx.x >> 5];
   const int nbig = ld(&ctl->nbig);
   // Long rows, ONE per warp claim: every long row in flight scans its
-  // higher-priority list concurrently, so when its last dependency is
-  // coloured only that entry remains (a warp holding several would scan
-  // them one after another, on the critical path of the dense hub core).
+  // higher-priority list concurrently, so the dense hub core's rows all wait
+  // at the same time instead of one after another.
   while (true) {
     int r = 0;
     if (lane == 0) r = fetch_add(&ctl->head_big, 1);
@@ -234,36 +381,8 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
     if (r >= nbig) break;
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
-    const int we = wb + __ldg(&hc[wv]);
-    int off = 0, c = -1;
-    while (c < 0) {
-      bits[lane] = 0;
-      bits[lane + 32] = 0;
-      __syncwarp();
-      bool stalled = false;
-      for (int i = wb + lane; i < we; i += 32) {
-        const int cu = gc_wait_colour(color, __ldg(&nl2[i]), status);
-        if (cu < 0) {
-          stalled = true;
-          break;
-        }
-        const int d = cu - off;
-        if (d >= 0 && d < 32 * kMexWords) atomicOr(&bits[d >> 5], 1u << (d & 31));
-      }
-      if (__any_sync(kFull, stalled)) return;
-      __syncwarp();
-      const unsigned w0 = bits[lane], w1 = bits[lane + 32];
-      const unsigned f0 = __ballot_sync(kFull, w0 != ~0u), f1 = __ballot_sync(kFull, w1 != ~0u);
-      if (f0) {
-        const int wi = __ffs(f0) - 1;
-        c = off + wi * 32 + __ffs(~__shfl_sync(kFull, w0, wi)) - 1;
-      } else if (f1) {
-        const int wi = __ffs(f1) - 1;
-        c = off + (wi + 32) * 32 + __ffs(~__shfl_sync(kFull, w1, wi)) - 1;
-      }
-      __syncwarp();
-      off += 32 * kMexWords;
-    }
+    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, status);
+    if (c < 0) return;
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
   }
@@ -274,25 +393,10 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
     base = __shfl_sync(kFull, base, 0);
     if (base >= n) return;
     const int r = base + lane;
-    int v = -1, beg = 0, h = 0;
     if (r < n) {
-      v = __ldg(&order[r]);
-      beg = __ldg(&nindex[v]);
-      h = __ldg(&hc[v]);
-    }
-    // colour <= h <= 32: one 64-bit mask
-    if (v >= 0) {
-      unsigned long long used = 0;
-      bool ok = true;
-      for (int i = beg; i < beg + h; i++) {
-        const int cu = gc_wait_colour(color, __ldg(&nl2[i]), status);
-        if (cu < 0) {
-          ok = false;
-          break;
-        }
-        if (cu < 64) used |= 1ull << cu;
-      }
-      if (ok) st(&color[v], __ffsll((long long)~used) - 1);
+      const int v = __ldg(&order[r]);
+      const int c = gc_short_row(__ldg(&nindex[v]), __ldg(&hc[v]), nl2, color, status);
+      if (c >= 0) st(&color[v], c);
     }
     if (__any_sync(kFull, ld(&status->code) != 0)) return;
   }
