@@ -33,6 +33,7 @@ using namespace dev;
 
 constexpr int kTPB = 256;
 constexpr int kLaneMax = 32;
+constexpr int kBatch = 4;  // list entries per lane whose loads are issued together
 constexpr unsigned kIn = 0xfe;
 
 __device__ __forceinline__ unsigned byte_of(unsigned word, int v) { return (word >> ((v & 3) * 8)) & 0xffu; }
@@ -140,16 +141,24 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
       int verdict = kWait;
       if (und && !big) {
         verdict = kJoin;
-        for (int i = beg; i < end; i++) {
-          const int u = __ldg(&nlist[i]);
-          if ((unsigned)u >= (unsigned)n || u == v) {  // out of range, or a self-loop
-            raise(status, ECL_ERR_BAD_GRAPH, u);
-            continue;
-          }
-          const int r = mis_verdict(byte_of(ld(&st4[u >> 2]), u), b, u, v);
-          if (r != kJoin) {
-            verdict = r;
-            break;
+        // kBatch entries at a time: their index loads, then their status
+        // loads, are all in flight before the first verdict is needed
+        for (int i0 = beg; i0 < end && verdict == kJoin; i0 += kBatch) {
+          int u[kBatch];
+          unsigned w[kBatch];
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) u[k] = i0 + k < end ? __ldg(&nlist[i0 + k]) : -1;
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) w[k] = (unsigned)u[k] < (unsigned)n ? ld(&st4[u[k] >> 2]) : 0u;
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            if (i0 + k >= end || verdict != kJoin) continue;
+            if ((unsigned)u[k] >= (unsigned)n || u[k] == v) {  // out of range, or a self-loop
+              raise(status, ECL_ERR_BAD_GRAPH, u[k]);
+              continue;
+            }
+            const int r = mis_verdict(byte_of(w[k], u[k]), b, u[k], v);
+            if (r != kJoin) verdict = r;
           }
         }
         if (verdict == kJoin) {
@@ -173,22 +182,33 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
         const int wend = __shfl_sync(kFull, end, who);
         const unsigned wb = __shfl_sync(kFull, b, who);
         int wverdict = kJoin;
-        for (int i0 = wbeg; i0 < wend; i0 += 32) {
-          const int i = i0 + lane;
-          int r = kJoin;
-          if (i < wend) {
-            const int u = __ldg(&nlist[i]);
-            if ((unsigned)u < (unsigned)n && u != wv) {
-              r = mis_verdict(byte_of(ld(&st4[u >> 2]), u), wb, u, wv);
+        for (int i0 = wbeg; i0 < wend; i0 += 32 * kBatch) {
+          int u[kBatch];
+          unsigned w[kBatch];
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            const int i = i0 + 32 * k + lane;
+            u[k] = i < wend ? __ldg(&nlist[i]) : -1;
+          }
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) w[k] = (unsigned)u[k] < (unsigned)n ? ld(&st4[u[k] >> 2]) : 0u;
+          bool out = false, wait = false;
+#pragma unroll
+          for (int k = 0; k < kBatch; k++) {
+            if (i0 + 32 * k + lane >= wend) continue;
+            if ((unsigned)u[k] < (unsigned)n && u[k] != wv) {
+              const int r = mis_verdict(byte_of(w[k], u[k]), wb, u[k], wv);
+              out |= r == kOut;
+              wait |= r == kWait;
             } else {
-              raise(status, ECL_ERR_BAD_GRAPH, u);
+              raise(status, ECL_ERR_BAD_GRAPH, u[k]);
             }
           }
-          if (__any_sync(kFull, r == kOut)) {
+          if (__any_sync(kFull, out)) {
             wverdict = kOut;
             break;
           }
-          if (__any_sync(kFull, r == kWait)) {
+          if (__any_sync(kFull, wait)) {
             wverdict = kWait;
             break;
           }
