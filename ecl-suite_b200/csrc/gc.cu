@@ -200,8 +200,8 @@ __device__ __forceinline__ unsigned long long gc_now() {
 
 constexpr unsigned long long kStallNs = 2000000000ull;  // 2 s without progress -> give up
 constexpr int kMexWords = 64;                           // warp bitmap: 2048 colours per window
-constexpr int kPend = 512;                              // per-warp list of undecided entries
-constexpr int kBatch = 8;                               // entries per lane whose loads are in flight together
+constexpr int kPend = 1024;                             // per-warp list of undecided entries
+constexpr int kBatch = 16;                              // entries per lane whose loads are in flight together
 
 // Colour of u once it is published (bounded wait).  Returns -1 on a stall.
 __device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* status) {
