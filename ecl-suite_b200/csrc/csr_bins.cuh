@@ -60,7 +60,9 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
 // then sees one atomic per ~kCap entries instead of one per warp step --
 // appends from every warp of the grid to a single counter serialise in L2.
 // All lanes call push() and flush() together; flush() once more at the end.
-template <typename T, int kCap>
+// kStream: write the list with evict-first stores, for a list much larger
+// than L2 that must not push the per-vertex arrays out of it.
+template <typename T, int kCap, bool kStream = false>
 struct WarpStage {
   T* buf;         // this warp's kCap slots in shared memory
   int count = 0;  // warp-uniform
@@ -83,9 +85,12 @@ struct WarpStage {
     if (lane == 0) base = fetch_add(counter, count);
     base = __shfl_sync(kFull, base, 0);
     for (int i = lane; i < count; i += 32) {
-      if ((long long)base + i < cap)
-        out[base + i] = buf[i];
-      else
+      if ((long long)base + i < cap) {
+        if (kStream)
+          __stcs(&out[base + i], buf[i]);
+        else
+          out[base + i] = buf[i];
+      } else
         overflow = true;
     }
     __syncwarp();

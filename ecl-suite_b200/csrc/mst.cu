@@ -21,8 +21,11 @@
 //    (2 bounded grid barriers per round): phase A re-roots each edge, drops
 //    intra-component edges and atomicMin's its key into both roots; phase B
 //    joins every edge that is the minimum of one of its roots and flags it.
-//    minv is double-buffered so its reset rides along with phase A instead
-//    of costing a third barrier; per-round sizes live in a counter array, so
+//    Per warp, every root is found, reset, loaded and min-published once
+//    (__match_any_sync groups): late rounds give one giant component most of
+//    the edges, and per-edge accesses to its root would queue at one L2 slice.
+//    minv is double-buffered so its reset (a streaming pass over the
+//    vertices) rides along with phase A instead of costing a third barrier; per-round sizes live in a counter array, so
 //    no counter is ever reset concurrently with its use.
 #include <cooperative_groups.h>
 
@@ -50,7 +53,17 @@ struct MSTCtl {
   int filter;
   int pad;
   u64 total;
+  // %globaltimer when each pass started and after each of its barriers
+  // (phase A of round r ends at [2r + 1], phase B at [2r + 2]): a per-round
+  // time profile that costs one store per barrier.
+  u64 stamp[2][2 * kMaxRounds + 2];
 };
+
+__device__ __forceinline__ u64 mst_now() {
+  u64 t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ int mst_find(int v, int* parent) {
   int cur = ld(&parent[v]);
@@ -174,7 +187,10 @@ __device__ __forceinline__ bool mst_entry(bool valid, int v, int rv, int j, int 
 
 // Slots per warp in the shared-memory staging of worklist appends.
 constexpr int kStage = 128;
-typedef WarpStage<int4, kStage> Stage;
+// Worklists are 16 B per edge (100 MB each for R-MAT-22's light edges):
+// they are written and read with evict-first hints so parent[] and the key
+// arrays, which Boruvka reads at random, stay in L2.
+typedef WarpStage<int4, kStage, true> Stage;
 
 // More v<n entries than the worklist holds: an asymmetric graph flagged
 // symmetric.
@@ -277,6 +293,21 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
   mst_overflow(overflow, status);
 }
 
+// Lowers mcur[root] to the smallest (weight << 32 | j) key among the lanes
+// of the warp that hold `root` and keep their edge: one atomic per root per
+// warp.  Late rounds give one giant component most of the edges, and an
+// atomic (or load) per edge on its root would queue at one L2 slice.  All
+// lanes call.
+__device__ __forceinline__ void mst_publish(u64* mcur, int root, bool keep, int w, int j, int lane) {
+  const unsigned g = __match_any_sync(kFull, keep ? root : -1);
+  const unsigned wmin = __reduce_min_sync(g, keep ? (unsigned)w : 0xffffffffu);
+  const unsigned jmin = __reduce_min_sync(g, (keep && (unsigned)w == wmin) ? (unsigned)j : 0xffffffffu);
+  if (keep && lane == __ffs(g) - 1) {
+    const u64 key = ((u64)wmin << 32) | jmin;
+    if (ld(&mcur[root]) > key) fetch_min(&mcur[root], key);
+  }
+}
+
 // All Boruvka rounds of one pass.  wlA holds the pass's initial worklist
 // (size wlcount[pass][0]); rounds alternate wlA/wlB.
 __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __restrict__ wlA, int4* __restrict__ wlB,
@@ -285,12 +316,14 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
                                                     Status* __restrict__ status) {
   const int tid = blockIdx.x * kTPB + threadIdx.x;
   const int nthreads = gridDim.x * kTPB;
+  const int lane = threadIdx.x & 31;
   int* cnt = ctl->wlcount[pass];
   __shared__ int4 stage_buf[kTPB / 32][kStage];
   Stage stg{stage_buf[threadIdx.x >> 5]};
   bool overflow = false;
   u64 local = 0;
   int r = 0;
+  if (tid == 0) ctl->stamp[pass][0] = mst_now();
   for (; r < kMaxRounds; r++) {
     int4* in = (r & 1) ? wlB : wlA;
     int4* out = (r & 1) ? wlA : wlB;
@@ -302,44 +335,57 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     // phase A: re-root, drop intra-component edges, publish keys.  The trip
     // count is uniform across the grid so every warp step is converged for
     // the warp-aggregated append.
+    // clear the keys round r-1 published: a streaming pass over all
+    // vertices (a reset per edge would store to the giant component's word
+    // from every warp)
+    if (r > 0)
+      for (int v = tid; v < n; v += nthreads) st(&mprev[v], ~0ull);
     const int iters = (sz + nthreads - 1) / nthreads;
     for (int it = 0; it < iters; it++) {
       const int i = tid + it * nthreads;
-      int4 e = make_int4(0, 0, 0, 0);
-      bool keep = false;
+      const bool valid = i < sz;
+      const int4 e = valid ? __ldcs(&in[i]) : make_int4(-1, -1, 0, 0);
+      // one find per distinct endpoint per warp (the lanes holding it share
+      // the result)
+      const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
+      const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
       int ra = 0, rb = 0;
-      if (i < sz) {
-        e = in[i];
-        if (r > 0) {  // clear the keys round r-1 published on these roots
-          st(&mprev[e.x], ~0ull);
-          st(&mprev[e.y], ~0ull);
-        }
-        ra = mst_find(e.x, parent);
-        rb = mst_find(e.y, parent);
-        keep = ra != rb;
-      }
+      if (valid && lane == lx) ra = mst_find(e.x, parent);
+      if (valid && lane == ly) rb = mst_find(e.y, parent);
+      ra = __shfl_sync(kFull, ra, lx);
+      rb = __shfl_sync(kFull, rb, ly);
+      const bool keep = valid && ra != rb;
       stg.push(keep, make_int4(ra, rb, e.z, e.w), out, &cnt[r + 1], cap, overflow);
-      if (keep) {
-        const u64 key = ((u64)(unsigned)e.z << 32) | (unsigned)e.w;
-        if (ld(&mcur[ra]) > key) fetch_min(&mcur[ra], key);
-        if (ld(&mcur[rb]) > key) fetch_min(&mcur[rb], key);
-      }
+      mst_publish(mcur, ra, keep, e.z, e.w, lane);
+      mst_publish(mcur, rb, keep, e.z, e.w, lane);
     }
     stg.flush(out, &cnt[r + 1], cap, overflow);
     if (!grid_sync(&ctl->bar, status)) return;
+    if (tid == 0) ctl->stamp[pass][2 * r + 1] = mst_now();
     const int nsz = ld(&cnt[r + 1]);
     if (nsz == 0) break;
     // phase B: join along every edge that is the minimum of one of its roots
-    for (int i = tid; i < nsz; i += nthreads) {
-      const int4 e = out[i];
+    // (each root's key is loaded once per warp)
+    for (int i0 = tid - lane; i0 < nsz; i0 += nthreads) {
+      const int i = i0 + lane;
+      const bool valid = i < nsz;
+      const int4 e = valid ? __ldcs(&out[i]) : make_int4(-1, -1, 0, 0);
+      const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
+      const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
+      u64 kx = 0, ky = 0;
+      if (valid && lane == lx) kx = ld(&mcur[e.x]);
+      if (valid && lane == ly) ky = ld(&mcur[e.y]);
+      kx = __shfl_sync(kFull, kx, lx);
+      ky = __shfl_sync(kFull, ky, ly);
       const u64 key = ((u64)(unsigned)e.z << 32) | (unsigned)e.w;
-      if (key == ld(&mcur[e.x]) || key == ld(&mcur[e.y])) {
+      if (valid && (key == kx || key == ky)) {
         mst_join(e.x, e.y, parent);
         in_mst[e.w] = 1;  // each entry j is joined at most once: plain byte store
         local += (u64)(unsigned)e.z;
       }
     }
     if (!grid_sync(&ctl->bar, status)) return;
+    if (tid == 0) ctl->stamp[pass][2 * r + 2] = mst_now();
   }
   if (r == kMaxRounds) raise(status, ECL_ERR_NO_CONVERGENCE, pass);
   // per-block sum of the joined weights
