@@ -29,6 +29,11 @@ for name, res, args in [
     ("orc_mst", C.c_uint64, [C.c_int, C.c_int, _P, _P, _P, _P]),
     ("orc_scc", None, [C.c_int, C.c_int, _P, _P, _P]),
     ("orc_apsp", None, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_long]),
+    ("omp_cc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("omp_mis", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("omp_gc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("omp_scc", None, [C.c_int, C.c_int, _P, _P, _P]),
+    ("omp_threads", C.c_int, []),
 ]:
     f = getattr(_lib, name)
     f.restype = res
@@ -114,3 +119,33 @@ def apsp(g) -> np.ndarray:
     out = np.empty((n, n), np.int32)
     _lib.orc_apsp(n, m, ni.ctypes.data, nl.ctypes.data, w.ctypes.data, out.ctypes.data, n)
     return out
+
+
+# ---- OpenMP CPU baselines (omp_baseline.c): same results, all host threads ----
+
+
+def omp_threads() -> int:
+    return int(_lib.omp_threads())
+
+
+def _omp(name, g, dtype):
+    n, m, ni, nl = _arrs(g)
+    out = np.empty(n, dtype)
+    getattr(_lib, name)(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def omp_cc(g) -> np.ndarray:
+    return _omp("omp_cc", g, np.int32)
+
+
+def omp_mis(g) -> np.ndarray:
+    return _omp("omp_mis", g, np.uint8)
+
+
+def omp_gc(g) -> np.ndarray:
+    return _omp("omp_gc", g, np.int32)
+
+
+def omp_scc(g) -> np.ndarray:
+    return _omp("omp_scc", g, np.int32)

@@ -71,3 +71,25 @@ def test_apsp_hand(orc):
     # a self-loop overwrites the 0 diagonal (init2, ECL-APSP-atomic.cu:79)
     s = from_edges(2, [(0, 0), (0, 1)], weights=[4, 1])
     assert orc.apsp(s)[0, 0] == 4
+
+
+def _omp_graphs(ecl):
+    return [
+        ecl.gen_rmat(14, 16, seed=2),
+        ecl.gen_rmat(13, 8, seed=9, symmetrise=False),
+        ecl.gen_grid(120, 90, 0.2, seed=3),
+        ecl.gen_er(3000, 0.003, seed=4, symmetrise=True),
+        undirected(2100, [(2099, i) for i in range(2099)] + [(i, i + 1) for i in range(0, 300, 2)]),
+    ]
+
+
+def test_openmp_baselines_match_the_serial_oracle(orc, ecl):
+    """The OpenMP CPU baselines (bench.py's CPU legs for CC, MIS, GC and SCC)
+    return exactly the serial oracle's results."""
+    assert orc.omp_threads() >= 1
+    for g in _omp_graphs(ecl):
+        assert np.array_equal(orc.omp_cc(g), orc.cc(g))
+        assert np.array_equal(orc.omp_scc(g), orc.scc(g))
+        if g.symmetric:
+            assert np.array_equal(orc.omp_mis(g), orc.mis(g))
+            assert np.array_equal(orc.omp_gc(g), orc.gc(g))
