@@ -32,6 +32,50 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
 CODES_SYM = ["cc", "mis", "gc", "mst"]
 
 
+# ---------------------------------------------------------------- ranks
+# One process per GPU (torchrun); every rank runs the same steps and the same
+# collectives in the same order.  A rate is the units ALL ranks processed
+# divided by the slowest rank's device time.
+
+
+def rank_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    """Largest x over all ranks (the identity on one rank)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, max_seconds):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units, timed by the slowest rank."""
+    return world * units_per_rank / max_seconds
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -197,6 +241,7 @@ def run_batch(args, rank, world, local_rank):
     tot_m = sum(g.edges for g in sizes)
     for _ in range(args.warmup):
         b.run()
+    rank_barrier(world)
     clk = Clocks(local_rank)
     clk.start()
     l0 = ecl.kernel_launches()
@@ -207,8 +252,10 @@ def run_batch(args, rank, world, local_rank):
         ms += t
         replay = replay and r
     launches = ecl.kernel_launches() - l0
+    rank_barrier(world)
     clocks = clk.stop()
-    value = G * args.steps / (ms / 1e3)
+    ms = max_over_ranks(ms, world)
+    value = job_rate(G * args.steps, world, ms / 1e3)
 
     # one graph per call, same solves, device-resident inputs
     dgs = [g.to_device(dev) for g in sizes]
@@ -238,8 +285,8 @@ def run_batch(args, rank, world, local_rank):
         plain(dg)
     ev1.record(stream)
     ev1.synchronize()
-    plain_ms = ev0.elapsed_time(ev1)
-    plain_gps = G / (plain_ms / 1e3)
+    plain_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    plain_gps = job_rate(G, world, plain_ms / 1e3)
     line = {
         "metric": "graphs/s (batched CC+MIS+MST over the 4096-graph mix; one CUDA-graph replay per step)",
         "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -310,6 +357,7 @@ def run_serve(args, rank, world, local_rank):
             gid = pool[int(rng.integers(0, len(pool)))][0]
             reqs.append((c, gid, t, None))
         print(f"serve: rate {rate} req/s, {count} requests", file=sys.stderr, flush=True)
+        rank_barrier(world)
         rc, arr, st = srv.run(reqs)
         print(f"serve: rate {rate} done rc={rc} p50={st.p50_s*1e3:.2f} ms p99={st.p99_s*1e3:.2f} ms "
               f"{st.graphs_per_s:.1f} graphs/s", file=sys.stderr, flush=True)
@@ -319,8 +367,14 @@ def run_serve(args, rank, world, local_rank):
             if lat:
                 per[names[c]] = {"p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                                  "n": len(lat)}
-        sweep.append({"rate_req_s": rate, "requests": count, "completed": st.completed, "failed": st.failed,
-                      "graphs_per_s": st.graphs_per_s, "p50_ms": 1e3 * st.p50_s, "p99_ms": 1e3 * st.p99_s,
+        # every rank serves its own stream: completions add up over the
+        # slowest rank's makespan; latency quantiles are the worst rank's
+        done = sum_over_ranks(st.completed, world)
+        makespan = max_over_ranks(st.makespan_s, world)
+        sweep.append({"rate_req_s": rate * world, "requests": count * world, "completed": int(done),
+                      "failed": int(sum_over_ranks(st.failed, world)),
+                      "graphs_per_s": done / makespan if makespan > 0 else 0.0,
+                      "p50_ms": 1e3 * max_over_ranks(st.p50_s, world), "p99_ms": 1e3 * max_over_ranks(st.p99_s, world),
                       "mean_ms": 1e3 * st.mean_s, "max_in_flight": st.max_in_flight,
                       "peak_gb": st.peak_bytes / 1e9, "per_code": per, "rc": rc})
     clocks = clk.stop()
@@ -424,8 +478,7 @@ def run_ours(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         step(False)
-    if world > 1:
-        torch.distributed.barrier()
+    rank_barrier(world)
     torch.cuda.synchronize()
     clk = Clocks(local_rank)
     clk.start()
@@ -435,8 +488,7 @@ def run_ours(args, rank, world, local_rank):
         total_ms += step(True)
     launches = ecl.kernel_launches() - l0
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    rank_barrier(world)
     clocks = clk.stop()
 
     is_apsp = jobs[0][0] == "apsp"
@@ -444,11 +496,8 @@ def run_ours(args, rank, world, local_rank):
     # n^3 relaxations for APSP (updates/s)
     units_step = float(jobs[0][1].nodes) ** 3 if is_apsp else sum(g.edges for _, g in jobs)
     unit = "updates/s" if is_apsp else "edges/s"
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * units_step * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, world)
+    value = job_rate(units_step * args.steps, world, total_ms / 1e3)
     ms_per_step = total_ms / args.steps
 
     # dominant kernel phase and its roofline
@@ -535,11 +584,8 @@ def run_ours(args, rank, world, local_rank):
             ev1.synchronize()
             if it > 0:  # first call warms the stream-ordered allocator
                 e_ms += ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([e_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": world * units_step * args.e2e_steps / (e_ms / 1e3), "unit": unit,
+        e_ms = max_over_ranks(e_ms, world)
+        e2e = {"value": job_rate(units_step * args.e2e_steps, world, e_ms / 1e3), "unit": unit,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": args.e2e_steps,
                "ms_per_step": e_ms / args.e2e_steps}
 
