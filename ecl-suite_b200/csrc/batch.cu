@@ -400,7 +400,7 @@ ecl_status ecl_batch_tune(ecl_batch* b, int32_t trials, ecl_tune* best) {
   using namespace ecl;
   if (!b || !b->built || trials < 1) return ECL_ERR_INVALID_ARG;
   const int bps[] = {4, 8};
-  const float light[] = {1.5f, 3.0f, 6.0f};
+  const float light[] = {0.75f, 1.5f, 3.0f};
   ecl_tune winner{};
   float best_ms = 1e30f;
   for (int x : bps) {

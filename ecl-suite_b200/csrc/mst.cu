@@ -10,7 +10,10 @@
 //
 // B200 design:
 //  * mst_threshold: one block samples 1024 weights on the device and picks
-//    the quantile that leaves ~1.5 n light edges (no host round trip);
+//    the quantile that leaves ~0.75 n light CSR entries (no host round
+//    trip).  Fewer light edges than the reference's 3n: on R-MAT-22 the light
+//    Boruvka pass then runs on ~1.6 M instead of ~6.4 M edges, and the
+//    flattened heavy pass absorbs the rest (factor 3 -> 0.75: MST 6.5 -> 5.0 ms);
 //  * mst_scan: builds a worklist of int4 {a, b, weight, j} from the CSR,
 //    lane-level for lists <= 32 entries, warp-level up to kChunk, chunk
 //    records beyond; appends are staged per warp in shared memory and
@@ -158,39 +161,68 @@ __device__ __forceinline__ bool mst_keep(int w, int thr) {
   return kLight ? (w <= thr) : (w > thr);
 }
 
-// Worklist entry for CSR entry j of vertex v (rv = v's root in the heavy
-// pass); returns whether it is kept.
-template <bool kLight>
-__device__ __forceinline__ bool mst_entry(bool valid, int v, int rv, int j, int n, const int* nlist, const int* eweight,
-                                          int thr, int* parent, int4& e, Status* status) {
-  if (!valid) return false;
-  const int u = __ldg(&nlist[j]);
-  if ((unsigned)u >= (unsigned)n) {
-    raise(status, ECL_ERR_BAD_GRAPH, u);
-    return false;
-  }
-  if (u <= v) return false;
-  const int w = __ldg(&eweight[j]);
-  if (w < 0) {
-    raise(status, ECL_ERR_BAD_GRAPH, j);
-    return false;
-  }
-  if (!mst_keep<kLight>(w, thr)) return false;
-  if (kLight) {
-    e = make_int4(v, u, w, j);
-    return true;
-  }
-  const int ru = ld(&parent[u]);  // flat after mst_flatten
-  e = make_int4(rv, ru, w, j);
-  return ru != rv;
-}
-
 // Slots per warp in the shared-memory staging of worklist appends.
 constexpr int kStage = 128;
 // Worklists are 16 B per edge (100 MB each for R-MAT-22's light edges):
 // they are written and read with evict-first hints so parent[] and the key
 // arrays, which Boruvka reads at random, stay in L2.
 typedef WarpStage<int4, kStage, true> Stage;
+
+// Entries per lane whose loads are issued together in the scans.
+constexpr int kScanBatch = 4;
+
+// Emits the worklist entries for kScanBatch CSR entries of vertex v per lane
+// (rv = v's root in the heavy pass): entry k of this lane is j0 + k * stride,
+// present when `active` and below jend.  All index loads, then the weight
+// loads of the v < u entries, then (heavy pass) their roots are in flight
+// together before any is used; every lane pushes kScanBatch times.
+template <bool kLight>
+__device__ __forceinline__ void mst_emit_batch(int j0, int stride, int jend, bool active, int v, int rv, int n,
+                                               const int* nlist, const int* eweight, int thr, const int* parent,
+                                               Stage& stg, int4* wl, int* cnt, int cap, bool& overflow,
+                                               Status* status) {
+  int u[kScanBatch], w[kScanBatch], ru[kScanBatch];
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    const int j = j0 + k * stride;
+    u[k] = (active && j < jend) ? __ldg(&nlist[j]) : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    const int j = j0 + k * stride;
+    w[k] = ((unsigned)u[k] < (unsigned)n && u[k] > v) ? __ldg(&eweight[j]) : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    ru[k] = (!kLight && (unsigned)u[k] < (unsigned)n && u[k] > v && mst_keep<false>(w[k], thr))
+                ? ld(&parent[u[k]])  // flat after mst_flatten
+                : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    const int j = j0 + k * stride;
+    bool keep = false;
+    int4 e = make_int4(0, 0, 0, 0);
+    if (active && j < jend) {
+      if ((unsigned)u[k] >= (unsigned)n) {
+        raise(status, ECL_ERR_BAD_GRAPH, u[k]);
+      } else if (u[k] > v) {
+        if (w[k] < 0) {
+          raise(status, ECL_ERR_BAD_GRAPH, j);
+        } else if (mst_keep<kLight>(w[k], thr)) {
+          if (kLight) {
+            keep = true;
+            e = make_int4(v, u[k], w[k], j);
+          } else {
+            keep = ru[k] != rv;
+            e = make_int4(rv, ru[k], w[k], j);
+          }
+        }
+      }
+    }
+    stg.push(keep, e, wl, cnt, cap, overflow);
+  }
+}
 
 // More v<n entries than the worklist holds: an asymmetric graph flagged
 // symmetric.
@@ -234,12 +266,9 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
     }
     // lane level: all lanes step through offset k together
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
-    for (int k = 0; k < kmax; k++) {
-      int4 e;
-      const bool keep = mst_entry<kLight>(lanelvl && k < deg, v, rv, beg + k, n, nlist, eweight, thr, parent, e,
-                                          status);
-      stg.push(keep, e, wl, cnt, cap, overflow);
-    }
+    for (int k0 = 0; k0 < kmax; k0 += kScanBatch)
+      mst_emit_batch<kLight>(beg + k0, 1, end, lanelvl, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                             overflow, status);
     // warp level
     unsigned todo = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
     while (todo) {
@@ -249,12 +278,9 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
       const int wrv = __shfl_sync(kFull, rv, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      for (int i0 = wbeg; i0 < wend; i0 += 32) {
-        int4 e;
-        const bool keep = mst_entry<kLight>(i0 + lane < wend, wv, wrv, i0 + lane, n, nlist, eweight, thr, parent, e,
-                                            status);
-        stg.push(keep, e, wl, cnt, cap, overflow);
-      }
+      for (int i0 = wbeg; i0 < wend; i0 += 32 * kScanBatch)
+        mst_emit_batch<kLight>(i0 + lane, 32, wend, true, wv, wrv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                               overflow, status);
     }
   }
   stg.flush(wl, cnt, cap, overflow);
@@ -282,12 +308,9 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
     const int v = rec.x;
     const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
     const int rv = kLight ? v : ld(&parent[v]);
-    for (int i0 = rec.y; i0 < end; i0 += 32) {
-      int4 e;
-      const bool keep = mst_entry<kLight>(i0 + lane < end, v, rv, i0 + lane, n, nlist, eweight, thr, parent, e,
-                                          status);
-      stg.push(keep, e, wl, cnt, cap, overflow);
-    }
+    for (int i0 = rec.y; i0 < end; i0 += 32 * kScanBatch)
+      mst_emit_batch<kLight>(i0 + lane, 32, end, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                             overflow, status);
   }
   stg.flush(wl, cnt, cap, overflow);
   mst_overflow(overflow, status);
@@ -440,7 +463,7 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
   if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));
   ECL_LAUNCH(mst_init, grid, kTPB, 0, stream, g.n, b.parent, b.minv);
   if (g.m > 0) {
-    const float light = dev.mst_light_factor > 0.f ? dev.mst_light_factor : 3.0f;
+    const float light = dev.mst_light_factor > 0.f ? dev.mst_light_factor : 0.75f;
     ECL_LAUNCH(mst_threshold, 1, kSamples, 0, stream, g.n, g.m, g.eweight, b.ctl, light);
     mark();
     for (int pass = 0; pass < 2; pass++) {
