@@ -68,16 +68,32 @@ __device__ __forceinline__ unsigned gc_h(const unsigned* vhash, int x) {
   return vhash ? __ldg(&vhash[x]) : ecl_hash((unsigned)x);
 }
 
-// 0: ignore (self-loop or invalid), 1: higher priority, 2: lower priority.
-__device__ __forceinline__ int gc_class(int u, int v, int dv, unsigned hv, int n, const int* nindex,
-                                        const unsigned* vhash, Status* status) {
-  if ((unsigned)u >= (unsigned)n) {
-    raise(status, ECL_ERR_BAD_GRAPH, u);
-    return 0;
+// Entries per lane whose loads are issued together in the init scans.
+constexpr int kInitBatch = 4;
+
+// Classes of kInitBatch list entries of v -- 0: ignore (self-loop or
+// invalid), 1: higher priority than v, 2: lower.  The list entries are loaded
+// first, then both row bounds of every neighbour, all before any is compared.
+__device__ __forceinline__ void gc_class_batch(const int (&u)[kInitBatch], const bool (&valid)[kInitBatch], int v,
+                                               int dv, unsigned hv, int n, const int* nindex, const unsigned* vhash,
+                                               Status* status, int (&cls)[kInitBatch]) {
+  int b[kInitBatch], e[kInitBatch];
+#pragma unroll
+  for (int k = 0; k < kInitBatch; k++) {
+    const bool ok = valid[k] && (unsigned)u[k] < (unsigned)n && u[k] != v;
+    b[k] = ok ? __ldg(&nindex[u[k]]) : 0;
+    e[k] = ok ? __ldg(&nindex[u[k] + 1]) : 0;
   }
-  if (u == v) return 0;
-  const int du = __ldg(&nindex[u + 1]) - __ldg(&nindex[u]);
-  return gc_outranks(du, gc_h(vhash, u), u, dv, hv, v) ? 1 : 2;
+#pragma unroll
+  for (int k = 0; k < kInitBatch; k++) {
+    cls[k] = 0;
+    if (!valid[k]) continue;
+    if ((unsigned)u[k] >= (unsigned)n) {
+      raise(status, ECL_ERR_BAD_GRAPH, u[k]);
+    } else if (u[k] != v) {
+      cls[k] = gc_outranks(e[k] - b[k], gc_h(vhash, u[k]), u[k], dv, hv, v) ? 1 : 2;
+    }
+  }
 }
 
 // vhash[v] = hash of v's local id in a union of graphs.
@@ -110,10 +126,18 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
     int h = 0;
     if (dv > kBinChunk) push_row_chunks(rc, v, beg, end);
     if (v < n && dv <= kBinLane) {
-      for (int i = beg; i < end; i++) {
-        const int u = __ldg(&nlist[i]);
-        const int k = gc_class(u, v, dv, hv, n, nindex, vhash, status);
-        if (k == 1) nl2[beg + h++] = u;
+      for (int i0 = beg; i0 < end; i0 += kInitBatch) {
+        int u[kInitBatch], cls[kInitBatch];
+        bool valid[kInitBatch];
+#pragma unroll
+        for (int k = 0; k < kInitBatch; k++) {
+          valid[k] = i0 + k < end;
+          u[k] = valid[k] ? __ldg(&nlist[i0 + k]) : 0;
+        }
+        gc_class_batch(u, valid, v, dv, hv, n, nindex, vhash, status, cls);
+#pragma unroll
+        for (int k = 0; k < kInitBatch; k++)
+          if (cls[k] == 1) nl2[beg + h++] = u[k];
       }
     }
     unsigned todo = __ballot_sync(kFull, dv > kBinLane && dv <= kBinChunk);
@@ -125,15 +149,21 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       const int wend = __shfl_sync(kFull, end, who);
       const unsigned whv = gc_h(vhash, wv);
       int wh = 0;
-      for (int i0 = wbeg; i0 < wend; i0 += 32) {
-        int k = 0, u = 0;
-        if (i0 + lane < wend) {
-          u = __ldg(&nlist[i0 + lane]);
-          k = gc_class(u, wv, wend - wbeg, whv, n, nindex, vhash, status);
+      for (int i0 = wbeg; i0 < wend; i0 += 32 * kInitBatch) {
+        int u[kInitBatch], cls[kInitBatch];
+        bool valid[kInitBatch];
+#pragma unroll
+        for (int k = 0; k < kInitBatch; k++) {
+          valid[k] = i0 + 32 * k + lane < wend;
+          u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
         }
-        const unsigned bh = __ballot_sync(kFull, k == 1);
-        if (k == 1) nl2[wbeg + wh + __popc(bh & ((1u << lane) - 1))] = u;
-        wh += __popc(bh);
+        gc_class_batch(u, valid, wv, wend - wbeg, whv, n, nindex, vhash, status, cls);
+#pragma unroll
+        for (int k = 0; k < kInitBatch; k++) {
+          const unsigned bh = __ballot_sync(kFull, cls[k] == 1);
+          if (cls[k] == 1) nl2[wbeg + wh + __popc(bh & ((1u << lane) - 1))] = u[k];
+          wh += __popc(bh);
+        }
       }
       if (lane == who) h = wh;
     }
@@ -156,17 +186,30 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
     const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
     const int stop = min(r.y + kBinChunk, end);
     const unsigned hv = gc_h(vhash, v);
-    for (int i0 = r.y; i0 < stop; i0 += 32) {
-      int k = 0, u = 0;
-      if (i0 + lane < stop) {
-        u = __ldg(&nlist[i0 + lane]);
-        k = gc_class(u, v, end - beg, hv, n, nindex, vhash, status);
+    for (int i0 = r.y; i0 < stop; i0 += 32 * kInitBatch) {
+      int u[kInitBatch], cls[kInitBatch];
+      bool valid[kInitBatch];
+#pragma unroll
+      for (int k = 0; k < kInitBatch; k++) {
+        valid[k] = i0 + 32 * k + lane < stop;
+        u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
       }
-      const unsigned bh = __ballot_sync(kFull, k == 1);
+      gc_class_batch(u, valid, v, end - beg, hv, n, nindex, vhash, status, cls);
+      unsigned bh[kInitBatch];
+      int total = 0;
+#pragma unroll
+      for (int k = 0; k < kInitBatch; k++) {
+        bh[k] = __ballot_sync(kFull, cls[k] == 1);
+        total += __popc(bh[k]);
+      }
       int hbase = 0;
-      if (lane == 0 && bh) hbase = fetch_add(&hc[v], __popc(bh));
+      if (lane == 0 && total) hbase = fetch_add(&hc[v], total);
       hbase = __shfl_sync(kFull, hbase, 0);
-      if (k == 1) nl2[beg + hbase + __popc(bh & ((1u << lane) - 1))] = u;
+#pragma unroll
+      for (int k = 0; k < kInitBatch; k++) {
+        if (cls[k] == 1) nl2[beg + hbase + __popc(bh[k] & ((1u << lane) - 1))] = u[k];
+        hbase += __popc(bh[k]);
+      }
     }
   }
 }

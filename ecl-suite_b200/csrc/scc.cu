@@ -40,6 +40,7 @@ using namespace dev;
 
 constexpr int kTPB = 256;
 constexpr int kMaxSweeps = 1 << 16;
+constexpr int kScanBatch = 4;  // list entries per lane whose loads are issued together
 
 struct SCCCtl {
   GridBarrier bar;
@@ -108,9 +109,12 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     bool out = false;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
-    for (int k = 0; k < kmax; k++) {
-      const bool valid = lanelvl && k < deg;
-      scc_mark_entry(valid, v, valid ? __ldg(&nlist[beg + k]) : 0, n, flags, out, status);
+    for (int k0 = 0; k0 < kmax; k0 += kScanBatch) {
+      int w[kScanBatch];
+#pragma unroll
+      for (int k = 0; k < kScanBatch; k++) w[k] = (lanelvl && k0 + k < deg) ? __ldg(&nlist[beg + k0 + k]) : 0;
+#pragma unroll
+      for (int k = 0; k < kScanBatch; k++) scc_mark_entry(lanelvl && k0 + k < deg, v, w[k], n, flags, out, status);
     }
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
@@ -120,7 +124,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       bool wout = false;
-      for (int i = wbeg + lane; i < wend; i += 32) scc_mark_entry(true, wv, __ldg(&nlist[i]), n, flags, wout, status);
+      for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) {
+        int w[kScanBatch];
+#pragma unroll
+        for (int k = 0; k < kScanBatch; k++) w[k] = i0 + 32 * k < wend ? __ldg(&nlist[i0 + 32 * k]) : 0;
+#pragma unroll
+        for (int k = 0; k < kScanBatch; k++) scc_mark_entry(i0 + 32 * k < wend, wv, w[k], n, flags, wout, status);
+      }
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
     if (v < n && deg <= kBinChunk && out) fetch_or(&flags[v], kHasOut);  // long rows: scc_mark_chunks
@@ -139,7 +149,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     const int2 r = rc.rec[c];
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
-    for (int i = r.y + lane; i < end; i += 32) scc_mark_entry(true, r.x, __ldg(&nlist[i]), n, flags, out, status);
+    for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) {
+      int w[kScanBatch];
+#pragma unroll
+      for (int k = 0; k < kScanBatch; k++) w[k] = i0 + 32 * k < end ? __ldg(&nlist[i0 + 32 * k]) : 0;
+#pragma unroll
+      for (int k = 0; k < kScanBatch; k++) scc_mark_entry(i0 + 32 * k < end, r.x, w[k], n, flags, out, status);
+    }
     if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
   }
 }
@@ -148,9 +164,25 @@ __device__ __forceinline__ bool scc_live(const int* flags, int v) {
   return ld(&flags[v]) == (kHasIn | kHasOut);
 }
 
-__device__ __forceinline__ int2 scc_slot(bool live_v, int v, int w, int n, const int* flags) {
-  const bool keep = live_v && w != v && (unsigned)w < (unsigned)n && scc_live(flags, w);
-  return keep ? make_int2(v, w) : make_int2(-1, -1);
+// Writes the edge-list slots of kScanBatch CSR entries of v per lane: entry
+// k is j0 + k * stride when below jend.  The list entries, then the flag words
+// of their targets, are loaded before any slot is written.
+__device__ __forceinline__ void scc_slots(int j0, int stride, int jend, bool live_v, int v, int n,
+                                          const int* nlist, const int* flags, int2* wl) {
+  int w[kScanBatch], f[kScanBatch];
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    const int j = j0 + k * stride;
+    w[k] = j < jend ? __ldg(&nlist[j]) : -1;
+  }
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++)
+    f[k] = (live_v && (unsigned)w[k] < (unsigned)n && w[k] != v) ? ld(&flags[w[k]]) : 0;
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    const int j = j0 + k * stride;
+    if (j < jend) wl[j] = f[k] == (kHasIn | kHasOut) ? make_int2(v, w[k]) : make_int2(-1, -1);
+  }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __restrict__ nindex,
@@ -172,9 +204,8 @@ __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __res
     const int deg = end - beg;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
-    for (int k = 0; k < kmax; k++) {
-      if (lanelvl && k < deg) wl[beg + k] = scc_slot(live, v, __ldg(&nlist[beg + k]), n, flags);
-    }
+    for (int k0 = 0; k0 < kmax; k0 += kScanBatch)
+      if (lanelvl) scc_slots(beg + k0, 1, end, live, v, n, nlist, flags, wl);
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
@@ -183,7 +214,7 @@ __global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __res
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       const bool wlive = __shfl_sync(kFull, live, who);
-      for (int i = wbeg + lane; i < wend; i += 32) wl[i] = scc_slot(wlive, wv, __ldg(&nlist[i]), n, flags);
+      for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) scc_slots(i0, 32, wend, wlive, wv, n, nlist, flags, wl);
     }
   }
 }
@@ -200,7 +231,7 @@ __global__ void __launch_bounds__(kTPB) scc_build_chunks(int n, const int* __res
     const int2 r = rc.rec[c];
     const bool live = scc_live(flags, r.x);
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
-    for (int i = r.y + lane; i < end; i += 32) wl[i] = scc_slot(live, r.x, __ldg(&nlist[i]), n, flags);
+    for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) scc_slots(i0, 32, end, live, r.x, n, nlist, flags, wl);
   }
 }
 
