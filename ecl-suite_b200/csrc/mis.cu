@@ -123,14 +123,24 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   int sweep = 0;
+  // Bit g: this warp's g-th vertex group is fully decided and is skipped
+  // without a load (groups beyond the 64th are re-read every sweep).  Late
+  // sweeps then cost only the groups that still wait, not one L2 round trip
+  // per group owned.
+  unsigned long long done = 0;
   for (;; sweep++) {
     bool missing = false;
-    for (int base = warp * 32; base < n; base += nwarps * 32) {
+    int gi = 0;
+    for (int base = warp * 32; base < n; base += nwarps * 32, gi++) {
+      if (gi < 64 && ((done >> gi) & 1ull)) continue;
       const int v = base + lane;
       unsigned b = 0;
       if (v < n) b = byte_of(ld(&st4[v >> 2]), v);
       const bool und = (b & 1u) != 0;
-      if (!__any_sync(kFull, und)) continue;
+      if (!__any_sync(kFull, und)) {
+        if (gi < 64) done |= 1ull << gi;
+        continue;
+      }
       int beg = 0, end = 0;
       if (und) {
         beg = __ldg(&nindex[v]);
