@@ -369,7 +369,9 @@ __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, uns
 // scheme with a bit mask of the undecided entries -- wait for the first one,
 // re-check the others without blocking.  -1 on a stall.
 __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, Status* status) {
-  unsigned long long used = 0;  // colour <= h <= 32
+  // colour <= h <= 32: a neighbour's colour of 64 or more (a hub's) cannot
+  // be the smallest free one and is left out of the mask
+  unsigned long long used = 0;
   unsigned pendm = 0;
   for (int k0 = 0; k0 < h; k0 += kBatch) {
     int u[kBatch], c[kBatch];
@@ -381,7 +383,7 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
     for (int k = 0; k < kBatch; k++) {
       if (u[k] < 0) continue;
       if (c[k] >= 0)
-        used |= 1ull << (c[k] & 63);
+        used |= c[k] < 64 ? 1ull << c[k] : 0ull;
       else
         pendm |= 1u << (k0 + k);
     }
@@ -390,13 +392,13 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
     const int k0 = __ffs(pendm) - 1;
     const int c0 = gc_wait_colour(color, __ldg(&nl2[beg + k0]), status);
     if (c0 < 0) return -1;
-    used |= 1ull << (c0 & 63);
+    used |= c0 < 64 ? 1ull << c0 : 0ull;
     pendm &= pendm - 1;
     for (unsigned mm = pendm; mm; mm &= mm - 1) {
       const int k = __ffs(mm) - 1;
       const int c = ld(&color[__ldg(&nl2[beg + k])]);
       if (c >= 0) {
-        used |= 1ull << (c & 63);
+        used |= c < 64 ? 1ull << c : 0ull;
         pendm &= ~(1u << k);
       }
     }

@@ -360,3 +360,79 @@ void orc_apsp(int n, int m, const int* nindex, const int* nlist, const int* ewei
       }
     }
 }
+
+/* Rows `rows[0..nrows)` of the same closure as orc_apsp, by Dijkstra from
+ * each requested source, for matrices too large for the O(n^3) restatement.
+ * The arc weight of (i, j) is the LAST list entry i -> j, as the matrix fill
+ * of ECL-APSP-atomic.cu:74-83 leaves it; the graph must have no self-loops
+ * (then the closure's diagonal is 0) and non-negative weights.  Unreachable
+ * entries are ORC_INF.  out is nrows x n. */
+void orc_apsp_rows(int n, int m, const int* nindex, const int* nlist, const int* eweight, const int* rows, int nrows,
+                   int* out) {
+  (void)m;
+  long long* d = (long long*)malloc(sizeof(long long) * (size_t)n);
+  int* heap = (int*)malloc(sizeof(int) * (size_t)(m + n + 1)); /* lazy-deletion heap of (vertex) keyed by d */
+  long long* hk = (long long*)malloc(sizeof(long long) * (size_t)(m + n + 1));
+  int* last = (int*)malloc(sizeof(int) * (size_t)n); /* entry index of the last i -> j, per j (scratch) */
+  for (int j = 0; j < n; j++) last[j] = -1;
+  for (int r = 0; r < nrows; r++) {
+    const int s = rows[r];
+    for (int j = 0; j < n; j++) d[j] = -1;
+    int hs = 0;
+    d[s] = 0;
+    heap[hs] = s;
+    hk[hs++] = 0;
+    while (hs > 0) {
+      /* pop min */
+      const int v = heap[0];
+      const long long dv = hk[0];
+      hs--;
+      heap[0] = heap[hs];
+      hk[0] = hk[hs];
+      for (int i = 0;;) {
+        int c = 2 * i + 1;
+        if (c >= hs) break;
+        if (c + 1 < hs && hk[c + 1] < hk[c]) c++;
+        if (hk[c] >= hk[i]) break;
+        const int tv = heap[i];
+        const long long tk = hk[i];
+        heap[i] = heap[c];
+        hk[i] = hk[c];
+        heap[c] = tv;
+        hk[c] = tk;
+        i = c;
+      }
+      if (dv > d[v] && d[v] >= 0) continue; /* stale */
+      /* last duplicate of each arc wins */
+      for (int e = nindex[v]; e < nindex[v + 1]; e++) last[nlist[e]] = e;
+      for (int e = nindex[v]; e < nindex[v + 1]; e++) {
+        const int u = nlist[e];
+        if (last[u] != e) continue;
+        const long long nd = dv + eweight[e];
+        if (d[u] < 0 || nd < d[u]) {
+          d[u] = nd;
+          int i = hs++;
+          heap[i] = u;
+          hk[i] = nd;
+          while (i > 0) {
+            const int p = (i - 1) / 2;
+            if (hk[p] <= hk[i]) break;
+            const int tv = heap[i];
+            const long long tk = hk[i];
+            heap[i] = heap[p];
+            hk[i] = hk[p];
+            heap[p] = tv;
+            hk[p] = tk;
+            i = p;
+          }
+        }
+      }
+      for (int e = nindex[v]; e < nindex[v + 1]; e++) last[nlist[e]] = -1;
+    }
+    for (int j = 0; j < n; j++) out[(long)r * n + j] = (d[j] < 0 || d[j] > ORC_INF) ? ORC_INF : (int)d[j];
+  }
+  free(d);
+  free(heap);
+  free(hk);
+  free(last);
+}

@@ -29,6 +29,7 @@ for name, res, args in [
     ("orc_mst", C.c_uint64, [C.c_int, C.c_int, _P, _P, _P, _P]),
     ("orc_scc", None, [C.c_int, C.c_int, _P, _P, _P]),
     ("orc_apsp", None, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_long]),
+    ("orc_apsp_rows", None, [C.c_int, C.c_int, _P, _P, _P, _P, C.c_int, _P]),
     ("omp_cc", None, [C.c_int, C.c_int, _P, _P, _P]),
     ("omp_mis", None, [C.c_int, C.c_int, _P, _P, _P]),
     ("omp_gc", None, [C.c_int, C.c_int, _P, _P, _P]),
@@ -110,6 +111,16 @@ def scc(g) -> np.ndarray:
     n, m, ni, nl = _arrs(g)
     out = np.empty(n, np.int32)
     _lib.orc_scc(n, m, ni.ctypes.data, nl.ctypes.data, out.ctypes.data)
+    return out
+
+
+def apsp_rows(g, rows) -> np.ndarray:
+    """Rows of the APSP closure by Dijkstra (no self-loops; last duplicate wins)."""
+    n, m, ni, nl = _arrs(g)
+    w = np.ascontiguousarray(g.eweight, dtype=np.int32) if m else np.zeros(1, np.int32)
+    r = np.ascontiguousarray(rows, dtype=np.int32)
+    out = np.empty((r.size, n), np.int32)
+    _lib.orc_apsp_rows(n, m, ni.ctypes.data, nl.ctypes.data, w.ctypes.data, r.ctypes.data, int(r.size), out.ctypes.data)
     return out
 
 

@@ -93,3 +93,14 @@ def test_openmp_baselines_match_the_serial_oracle(orc, ecl):
         if g.symmetric:
             assert np.array_equal(orc.omp_mis(g), orc.mis(g))
             assert np.array_equal(orc.omp_gc(g), orc.gc(g))
+
+
+def test_apsp_rows_match_the_closure(orc, ecl):
+    """Dijkstra rows (used at full size) equal rows of the FW restatement."""
+    for g in [ecl.gen_er(300, 0.02, seed=4, weight_seed=5), ecl.gen_er(257, 0.05, seed=9, weight_seed=2)]:
+        full = orc.apsp(g)
+        rows = np.array([0, 7, 100, g.nodes - 1], np.int32)
+        assert np.array_equal(orc.apsp_rows(g, rows), full[rows])
+    # duplicates: the last entry of an arc wins, as in the matrix fill
+    d = from_edges(3, [(0, 1), (0, 1), (1, 2)], weights=[9, 4, 2])
+    assert np.array_equal(orc.apsp_rows(d, np.array([0])), orc.apsp(d)[[0]])

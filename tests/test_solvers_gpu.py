@@ -85,6 +85,25 @@ def test_gc_large_colour_windows(ecl, orc):
 # ------------------------------------------------------------------------- MST
 
 
+def test_gc_short_row_ignores_colours_above_its_range(ecl, orc):
+    """A row of <= 32 entries (one lane) whose higher neighbour is a hub with
+    colour 64 or more: that colour cannot be its smallest free one and must
+    not stand for a low colour (64 would alias 0 in a 64-bit mask).  A
+    70-clique with one pendant vertex on every member: the members keep equal
+    degrees, so their colours run 0..69, and every pendant of a member
+    coloured 1..69 takes colour 0."""
+    n = 70
+    edges = [(i, j) for i in range(n) for j in range(i + 1, n)] + [(i, n + i) for i in range(n)]
+    g = undirected(2 * n, edges)
+    got = ecl.gc(g)
+    exp = orc.gc(g)
+    assert np.array_equal(got, exp)
+    assert sorted(got[:n]) == list(range(n))
+    for i in range(n):
+        if got[i] >= 64:
+            assert got[n + i] == 0
+
+
 def test_mst_matches_kruskal(ecl, orc):
     for name, g in sym_cases(ecl):
         g = weighted(g)
