@@ -7,6 +7,7 @@
   host time here, MST's Kruskal most of it.
 - APSP on ER n=8192.  An O(n^3) host closure would take hours, so
   32 random rows are checked exactly against Dijkstra from those sources.
+- the batched 4096-graph mix, 16 sampled graphs against the oracle.
 """
 import numpy as np
 import pytest
@@ -57,3 +58,22 @@ def test_apsp_er8192_sampled_rows(ecl, orc):
     rows = np.random.default_rng(7).choice(g.nodes, 32, replace=False).astype(np.int32)
     assert np.array_equal(dist[rows], orc.apsp_rows(g, rows))
     assert np.all(np.diag(dist) == 0)
+
+
+def test_batch4096_sampled_graphs(ecl, orc):
+    """the 4096-graph mix (about 1.4 G CSR entries in 3
+    super-batches), CC+MIS+MST on a CUDA-graph replay; 16 sampled graphs are
+    checked against the oracle."""
+    b = ecl.Batch()
+    b.add_mix(4096, n_min=1000, n_max=200000, seed=5, weight_max=1 << 16)
+    b.build(ecl.BATCH_CC | ecl.BATCH_MIS | ecl.BATCH_MST)
+    b.run()
+    _, replay = b.run()
+    assert replay
+    for i in np.random.default_rng(3).choice(b.graphs, 16, replace=False):
+        g = b.graph(int(i))
+        assert np.array_equal(b.result(int(i), ecl.BATCH_CC), orc.cc(g)), i
+        assert np.array_equal(b.result(int(i), ecl.BATCH_MIS), orc.mis(g)), i
+        inm, tot = b.result(int(i), ecl.BATCH_MST)
+        einm, etot = orc.mst(g)
+        assert tot == etot and np.array_equal(inm, einm), i
