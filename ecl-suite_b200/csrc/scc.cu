@@ -79,14 +79,26 @@ __device__ __forceinline__ bool io_raise(unsigned long long* p, unsigned long lo
 // with such an entry; rows longer than kBinChunk go to chunk records.
 constexpr int kHasIn = 1, kHasOut = 2;
 
-__device__ __forceinline__ void scc_mark_entry(bool valid, int v, int w, int n, int* flags, bool& out,
-                                               Status* status) {
-  if (!valid) return;
-  if ((unsigned)w >= (unsigned)n) {
-    raise(status, ECL_ERR_BAD_GRAPH, w);
-  } else if (w != v) {
-    fetch_or(&flags[w], kHasIn);
-    out = true;
+// Marks kScanBatch entries w[k] (present where valid[k]) of v's list: v has
+// an out-entry and each w an in-entry (self-loops ignored).  The flag words
+// are read first and OR'ed only where kHasIn is still clear: R-MAT sends a
+// large share of all entries to a few hub ids, whose words would otherwise
+// take an atomic from every one of them.
+__device__ __forceinline__ void scc_mark_batch(const bool (&valid)[kScanBatch], int v, const int (&w)[kScanBatch],
+                                               int n, int* flags, bool& out, Status* status) {
+  int f[kScanBatch];
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++)
+    f[k] = (valid[k] && (unsigned)w[k] < (unsigned)n && w[k] != v) ? ld(&flags[w[k]]) : kHasIn;
+#pragma unroll
+  for (int k = 0; k < kScanBatch; k++) {
+    if (!valid[k]) continue;
+    if ((unsigned)w[k] >= (unsigned)n) {
+      raise(status, ECL_ERR_BAD_GRAPH, w[k]);
+    } else if (w[k] != v) {
+      if (!(f[k] & kHasIn)) fetch_or(&flags[w[k]], kHasIn);
+      out = true;
+    }
   }
 }
 
@@ -111,10 +123,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch) {
       int w[kScanBatch];
+      bool valid[kScanBatch];
 #pragma unroll
-      for (int k = 0; k < kScanBatch; k++) w[k] = (lanelvl && k0 + k < deg) ? __ldg(&nlist[beg + k0 + k]) : 0;
-#pragma unroll
-      for (int k = 0; k < kScanBatch; k++) scc_mark_entry(lanelvl && k0 + k < deg, v, w[k], n, flags, out, status);
+      for (int k = 0; k < kScanBatch; k++) {
+        valid[k] = lanelvl && k0 + k < deg;
+        w[k] = valid[k] ? __ldg(&nlist[beg + k0 + k]) : 0;
+      }
+      scc_mark_batch(valid, v, w, n, flags, out, status);
     }
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
@@ -126,10 +141,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       bool wout = false;
       for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) {
         int w[kScanBatch];
+        bool valid[kScanBatch];
 #pragma unroll
-        for (int k = 0; k < kScanBatch; k++) w[k] = i0 + 32 * k < wend ? __ldg(&nlist[i0 + 32 * k]) : 0;
-#pragma unroll
-        for (int k = 0; k < kScanBatch; k++) scc_mark_entry(i0 + 32 * k < wend, wv, w[k], n, flags, wout, status);
+        for (int k = 0; k < kScanBatch; k++) {
+          valid[k] = i0 + 32 * k < wend;
+          w[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k]) : 0;
+        }
+        scc_mark_batch(valid, wv, w, n, flags, wout, status);
       }
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
@@ -151,10 +169,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     bool out = false;
     for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) {
       int w[kScanBatch];
+      bool valid[kScanBatch];
 #pragma unroll
-      for (int k = 0; k < kScanBatch; k++) w[k] = i0 + 32 * k < end ? __ldg(&nlist[i0 + 32 * k]) : 0;
-#pragma unroll
-      for (int k = 0; k < kScanBatch; k++) scc_mark_entry(i0 + 32 * k < end, r.x, w[k], n, flags, out, status);
+      for (int k = 0; k < kScanBatch; k++) {
+        valid[k] = i0 + 32 * k < end;
+        w[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k]) : 0;
+      }
+      scc_mark_batch(valid, r.x, w, n, flags, out, status);
     }
     if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
   }
