@@ -116,6 +116,28 @@ __device__ __forceinline__ bool mis_claim(unsigned* st4, int v, unsigned b) {
 
 __device__ __forceinline__ void mis_set_out(unsigned* st4, int u) { fetch_and(&st4[u >> 2], ~(0xffu << ((u & 3) * 8))); }
 
+// A joined vertex sets its list entries nlist[i], i = i0, i0 + step, ...
+// below end, out.  Their status words are read first (kBatch at a time) and
+// only the entries not out yet take the atomic: a low-degree vertex that
+// joins mostly neighbours hubs, whose words would otherwise take one atomic
+// per joining neighbour.
+__device__ __forceinline__ void mis_clear_list(unsigned* st4, const int* nlist, int i0, int end, int step, int n) {
+  for (; i0 < end; i0 += step * kBatch) {
+    int u[kBatch];
+    unsigned w[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) {
+      const int i = i0 + k * step;
+      u[k] = i < end ? __ldg(&nlist[i]) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; k++) w[k] = (unsigned)u[k] < (unsigned)n ? ld(&st4[u[k] >> 2]) : 0u;
+#pragma unroll
+    for (int k = 0; k < kBatch; k++)
+      if ((unsigned)u[k] < (unsigned)n && byte_of(w[k], u[k]) != 0) mis_set_out(st4, u[k]);
+  }
+}
+
 __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, unsigned* __restrict__ st4,
                                                 Status* __restrict__ status, int max_sweeps) {
@@ -172,12 +194,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
           }
         }
         if (verdict == kJoin) {
-          if (mis_claim(st4, v, b)) {
-            for (int i = beg; i < end; i++) {
-              const int u = __ldg(&nlist[i]);
-              if ((unsigned)u < (unsigned)n) mis_set_out(st4, u);
-            }
-          }
+          if (mis_claim(st4, v, b)) mis_clear_list(st4, nlist, beg, end, 1, n);
         } else if (verdict == kOut) {
           mis_set_out(st4, v);
         }
@@ -226,12 +243,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
         if (wverdict == kJoin) {
           bool claimed = false;
           if (lane == 0) claimed = mis_claim(st4, wv, wb);
-          if (__shfl_sync(kFull, claimed, 0)) {
-            for (int i = wbeg + lane; i < wend; i += 32) {
-              const int u = __ldg(&nlist[i]);
-              if ((unsigned)u < (unsigned)n) mis_set_out(st4, u);
-            }
-          }
+          if (__shfl_sync(kFull, claimed, 0)) mis_clear_list(st4, nlist, wbeg + lane, wend, 32, n);
         } else if (wverdict == kOut && lane == 0) {
           mis_set_out(st4, wv);
         }
