@@ -416,14 +416,17 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   unsigned* bits = s_bits[threadIdx.x >> 5];
   int* pend = s_pend[threadIdx.x >> 5];
   const int nbig = ld(&ctl->nbig);
-  // Long rows, ONE per warp claim: every long row in flight scans its
+  const int gwarp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  // Ranks are dealt to warps round-robin and each warp takes its own in
+  // increasing order -- no shared claim counter (one atomic per row on a
+  // single word would serialise ~10^6 claims in L2).  Still deadlock-free:
+  // the warp holding the lowest unfinished rank is working on it, and all of
+  // that vertex's dependencies have lower ranks.
+  // Long rows, ONE per warp at a time: every long row in flight scans its
   // higher-priority list concurrently, so the dense hub core's rows all wait
   // at the same time instead of one after another.
-  while (true) {
-    int r = 0;
-    if (lane == 0) r = fetch_add(&ctl->head_big, 1);
-    r = __shfl_sync(kFull, r, 0);
-    if (r >= nbig) break;
+  for (int r = gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
     const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, status);
@@ -431,12 +434,8 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
   }
-  // Short rows: 32 ranks per claim, every lane its own vertex.
-  while (true) {
-    int base = 0;
-    if (lane == 0) base = nbig + fetch_add(&ctl->head_small, 32);
-    base = __shfl_sync(kFull, base, 0);
-    if (base >= n) return;
+  // Short rows: 32 consecutive ranks per warp step, every lane its own vertex.
+  for (int base = nbig + gwarp * 32; base < n; base += nwarps * 32) {
     const int r = base + lane;
     if (r < n) {
       const int v = __ldg(&order[r]);
