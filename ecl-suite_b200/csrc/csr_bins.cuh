@@ -35,11 +35,27 @@ __device__ __forceinline__ void csr_row(const int* nindex, int v, int m, int& be
   }
 }
 
-// Called by the lane that owns a long row.
-__device__ __forceinline__ void push_row_chunks(RowChunks rc, int v, int beg, int end) {
-  const int nc = (end - beg + kBinChunk - 1) / kBinChunk;
-  const int at = fetch_add(rc.count, nc);
-  for (int c = 0; c < nc; c++) rc.rec[at + c] = make_int2(v, beg + c * kBinChunk);
+// Chunk records for the long rows of a warp's 32 vertices: every lane of the
+// warp calls; lanes with `is_long` cut [beg, end) into kChunkLen-entry
+// records (vertex, first entry).  One atomic per warp reserves all of them
+// (R-MAT-22 has ~50k rows over 256 entries; an atomic per row on one counter
+// would serialise in L2); the records land in lane order.
+template <int kChunkLen>
+__device__ __forceinline__ void push_chunks_warp(int2* rec, int* count, bool is_long, int v, int beg, int end) {
+  const int lane = threadIdx.x & 31;
+  const int nc = is_long ? (end - beg + kChunkLen - 1) / kChunkLen : 0;
+  if (!__any_sync(kFull, nc > 0)) return;
+  int incl = nc;  // inclusive prefix sum over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int total = __shfl_sync(kFull, incl, 31);
+  int base = 0;
+  if (lane == 0) base = fetch_add(count, total);
+  base = __shfl_sync(kFull, base, 0) + incl - nc;
+  for (int c = 0; c < nc; c++) rec[base + c] = make_int2(v, beg + c * kChunkLen);
 }
 
 // Warp-aggregated slot in an append-only list; every lane of the warp calls.

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
     const int dv = end - beg;
     const unsigned hv = (v < n) ? gc_h(vhash, v) : 0u;
     int h = 0;
-    if (dv > kBinChunk) push_row_chunks(rc, v, beg, end);
+    push_chunks_warp<kBinChunk>(rc.rec, rc.count, dv > kBinChunk, v, beg, end);
     if (v < n && dv <= kBinLane) {
       for (int i0 = beg; i0 < end; i0 += kInitBatch) {
         int u[kInitBatch], cls[kInitBatch];
@@ -220,6 +220,11 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
 __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ nindex,
                                                 unsigned long long* __restrict__ keys, int* __restrict__ vals,
                                                 const unsigned* __restrict__ vhash, GCCtl* __restrict__ ctl) {
+  // rows longer than kWarpRow are counted per block and added once per block
+  __shared__ int s_big;
+  if (threadIdx.x == 0) s_big = 0;
+  __syncthreads();
+  int nb = 0;
   for (int base = (blockIdx.x * kTPB + threadIdx.x) & ~31; base < n; base += gridDim.x * kTPB) {
     const int i = base + (threadIdx.x & 31);
     bool big = false;
@@ -230,9 +235,11 @@ __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ n
       vals[i] = v;
       big = deg > (unsigned)kWarpRow;
     }
-    const int nb = __popc(__ballot_sync(kFull, big));
-    if ((threadIdx.x & 31) == 0 && nb) fetch_add(&ctl->nbig, nb);
+    nb += __popc(__ballot_sync(kFull, big));
   }
+  if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&s_big, nb);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_big) fetch_add(&ctl->nbig, s_big);
 }
 
 __device__ __forceinline__ unsigned long long gc_now() {

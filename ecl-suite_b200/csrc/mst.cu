@@ -259,11 +259,8 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
     const bool lanelvl = deg > 0 && deg <= kLaneMax;
     int rv = v;
     if (!kLight && deg > 0 && v < n) rv = ld(&parent[v]);
-    if (kLight && deg > kChunk) {  // chunk records are built once, in the light pass
-      const int nc = (deg + kChunk - 1) / kChunk;
-      const int at = fetch_add(&ctl->nchunks, nc);
-      for (int c = 0; c < nc; c++) chunks[at + c] = make_int2(v, beg + c * kChunk);
-    }
+    if (kLight)  // chunk records are built once, in the light pass
+      push_chunks_warp<kChunk>(chunks, &ctl->nchunks, deg > kChunk, v, beg, end);
     // lane level: all lanes step through offset k together
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch)

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       io[v] = io_pack(v, v);
     }
     const int deg = end - beg;
-    if (deg > kBinChunk) push_row_chunks(rc, v, beg, end);
+    push_chunks_warp<kBinChunk>(rc.rec, rc.count, deg > kBinChunk, v, beg, end);
     bool out = false;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
