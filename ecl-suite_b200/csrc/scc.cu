@@ -282,6 +282,12 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restric
         return;
       }
       bool moved = false;
+      // The jump targets converge on a few vertices (the largest SCC's
+      // maximum id first of all), so every thread keeps its last jump of
+      // each kind: a repeated target reuses the value instead of loading the
+      // same word as every other edge.  A value read earlier is a smaller
+      // but still valid bound (in-max and out-max only grow).
+      int c_iv = -1, c_in = -1, c_ow = -1, c_out = -1;
       // Whole warps step together: in CSR order neighbouring lanes mostly
       // share v, so the out-max raises of v are combined per warp
       // (__match_any_sync + max) into one atomic instead of up to 32 on one
@@ -296,9 +302,21 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restric
           A = ld(&io[v]);
           const unsigned long long B = ld(&io[w]);
           int iv = io_in(A);
-          if (iv != v) iv = max(iv, io_in(ld(&io[iv])));
+          if (iv != v) {
+            if (iv != c_iv) {
+              c_iv = iv;
+              c_in = io_in(ld(&io[iv]));
+            }
+            iv = max(iv, c_in);
+          }
           ow = io_out(B);
-          if (ow != w) ow = max(ow, io_out(ld(&io[ow])));
+          if (ow != w) {
+            if (ow != c_ow) {
+              c_ow = ow;
+              c_out = io_out(ld(&io[ow]));
+            }
+            ow = max(ow, c_out);
+          }
           if (io_raise<true>(&io[w], B, iv)) moved = true;
         }
         const unsigned grp = __match_any_sync(kFull, v);
