@@ -318,13 +318,26 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
 // warp.  Late rounds give one giant component most of the edges, and an
 // atomic (or load) per edge on its root would queue at one L2 slice.  All
 // lanes call.
-__device__ __forceinline__ void mst_publish(u64* mcur, int root, bool keep, int w, int j, int lane) {
+// One-entry memo of a per-thread lookup (key -> value); key -1 = empty.
+struct MstMemo {
+  int key = -1;
+  u64 val = 0;
+};
+
+// ... and the calling thread remembers the last root it published to with
+// the smallest key it has seen there (a key word only decreases), so a giant
+// root met again in the next iterations costs no load.
+__device__ __forceinline__ void mst_publish(u64* mcur, int root, bool keep, int w, int j, int lane, MstMemo& memo) {
   const unsigned g = __match_any_sync(kFull, keep ? root : -1);
   const unsigned wmin = __reduce_min_sync(g, keep ? (unsigned)w : 0xffffffffu);
   const unsigned jmin = __reduce_min_sync(g, (keep && (unsigned)w == wmin) ? (unsigned)j : 0xffffffffu);
   if (keep && lane == __ffs(g) - 1) {
     const u64 key = ((u64)wmin << 32) | jmin;
-    if (ld(&mcur[root]) > key) fetch_min(&mcur[root], key);
+    if (memo.key == root && memo.val <= key) return;
+    const u64 cur = ld(&mcur[root]);
+    if (cur > key) fetch_min(&mcur[root], key);
+    memo.key = root;
+    memo.val = cur < key ? cur : key;
   }
 }
 
@@ -361,6 +374,9 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     if (r > 0)
       for (int v = tid; v < n; v += nthreads) st(&mprev[v], ~0ull);
     const int iters = (sz + nthreads - 1) / nthreads;
+    // per-thread memos: roots cannot change during phase A (joins happen in
+    // phase B), so a remembered find is exact
+    MstMemo fx, fy, px, py;
     for (int it = 0; it < iters; it++) {
       const int i = tid + it * nthreads;
       const bool valid = i < sz;
@@ -370,14 +386,26 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
       const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
       const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
       int ra = 0, rb = 0;
-      if (valid && lane == lx) ra = mst_find(e.x, parent);
-      if (valid && lane == ly) rb = mst_find(e.y, parent);
+      if (valid && lane == lx) {
+        if (fx.key != e.x) {
+          fx.key = e.x;
+          fx.val = (u64)mst_find(e.x, parent);
+        }
+        ra = (int)fx.val;
+      }
+      if (valid && lane == ly) {
+        if (fy.key != e.y) {
+          fy.key = e.y;
+          fy.val = (u64)mst_find(e.y, parent);
+        }
+        rb = (int)fy.val;
+      }
       ra = __shfl_sync(kFull, ra, lx);
       rb = __shfl_sync(kFull, rb, ly);
       const bool keep = valid && ra != rb;
       stg.push(keep, make_int4(ra, rb, e.z, e.w), out, &cnt[r + 1], cap, overflow);
-      mst_publish(mcur, ra, keep, e.z, e.w, lane);
-      mst_publish(mcur, rb, keep, e.z, e.w, lane);
+      mst_publish(mcur, ra, keep, e.z, e.w, lane, px);
+      mst_publish(mcur, rb, keep, e.z, e.w, lane, py);
     }
     stg.flush(out, &cnt[r + 1], cap, overflow);
     if (!grid_sync(&ctl->bar, status)) return;
@@ -385,7 +413,9 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     const int nsz = ld(&cnt[r + 1]);
     if (nsz == 0) break;
     // phase B: join along every edge that is the minimum of one of its roots
-    // (each root's key is loaded once per warp)
+    // (each root's key is loaded once per warp, and key words do not change
+    // during phase B, so a per-thread memo of the last one is exact)
+    MstMemo kxm, kym;
     for (int i0 = tid - lane; i0 < nsz; i0 += nthreads) {
       const int i = i0 + lane;
       const bool valid = i < nsz;
@@ -393,8 +423,20 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
       const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
       const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
       u64 kx = 0, ky = 0;
-      if (valid && lane == lx) kx = ld(&mcur[e.x]);
-      if (valid && lane == ly) ky = ld(&mcur[e.y]);
+      if (valid && lane == lx) {
+        if (kxm.key != e.x) {
+          kxm.key = e.x;
+          kxm.val = ld(&mcur[e.x]);
+        }
+        kx = kxm.val;
+      }
+      if (valid && lane == ly) {
+        if (kym.key != e.y) {
+          kym.key = e.y;
+          kym.val = ld(&mcur[e.y]);
+        }
+        ky = kym.val;
+      }
       kx = __shfl_sync(kFull, kx, lx);
       ky = __shfl_sync(kFull, ky, ly);
       const u64 key = ((u64)(unsigned)e.z << 32) | (unsigned)e.w;
