@@ -14,14 +14,14 @@
 //  * gc_keys + radix_sort_pairs rank all vertices by priority (a stable LSD
 //    sort on the inverted (degree, hash) key over ids in descending order),
 //    which is a topological order of the colouring dependencies.
-//  * gc_pull is ONE cooperative persistent launch.  Warps claim ranks in that
-//    order -- one long row (> 32 entries; they form a prefix of the order,
-//    priority being degree-first) or 32 short rows at a time; each vertex
-//    waits (bounded polling of exactly its
-//    own higher-priority neighbours' colour words -- no shared hot spot) until
-//    they are coloured and stores the smallest colour they do not use.
-//    Because claims follow the topological order, the lowest unfinished rank
-//    always has all its dependencies finished, so the launch always makes
+//  * gc_pull is ONE cooperative persistent launch.  Ranks are dealt to the
+//    warps round-robin -- one long row (> 32 entries; they form a prefix of
+//    the order, priority being degree-first) or 32 short rows at a time --
+//    and every warp takes its own in increasing order; each vertex waits
+//    (bounded polling of exactly its own higher-priority neighbours' colour
+//    words) until they are coloured and stores the smallest colour they do
+//    not use.  The warp holding the lowest unfinished rank is working on it,
+//    and all its dependencies have lower ranks, so the launch always makes
 //    progress.  There is no push, no counter and no queue: the total work is
 //    one read of every higher-priority entry, and the longest priority chain
 //    (about 2700 vertices at R-MAT-22, most of it in the hub core) costs one
@@ -47,10 +47,6 @@ constexpr int kTPB = 256;
 constexpr int kWarpRow = 32;  // rows longer than this are coloured by a whole warp
 
 struct GCCtl {
-  int head_big;    // next rank to claim among the long rows, [0, nbig)
-  int pad0[31];
-  int head_small;  // next rank to claim among the short rows, [nbig, n)
-  int pad1[31];
   int nchunks;
   int nbig;        // rows longer than kWarpRow: a prefix of the priority order
   int pad2[30];
