@@ -104,19 +104,71 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
+    """SM clock and clock-event reasons sampled DURING the timed region.
+
+    An NVML thread samples every 10 ms (the suite's timed region is ~70 ms, too
+    short for nvidia-smi's start-up and 200 ms period), with one sample at
+    start(); the device is matched to the CUDA device by UUID.  Falls back to
+    nvidia-smi sampling when NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.samples = []
+        self.stop_evt = None
+        self.thread = None
         self.p = None
+        self.nv = None
+        try:
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            handle = None
+            for i in range(nv.nvmlDeviceGetCount()):
+                h = nv.nvmlDeviceGetHandleByIndex(i)
+                u = nv.nvmlDeviceGetUUID(h)
+                u = u.decode() if isinstance(u, bytes) else u
+                if u.replace("GPU-", "") == uuid.replace("GPU-", ""):
+                    handle = h
+            if handle is None:
+                handle = nv.nvmlDeviceGetHandleByIndex(index)
+            self.nv, self.h = nv, handle
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(handle, nv.NVML_CLOCK_SM))
+            self.bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        except Exception:
+            self.nv = None
+
+    def _sample(self):
+        nv, h = self.nv, self.h
+        mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        self.samples.append((mhz, [n for n, b in zip(self.NAMES, self.bits) if r & b]))
+
+    def _run(self):
+        while not self.stop_evt.wait(0.01):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def start(self):
+        if self.nv is not None:
+            import threading
+
+            self._sample()
+            self.stop_evt = threading.Event()
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+            return
         try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
@@ -124,6 +176,13 @@ class Clocks:
             self.p = None
 
     def stop(self):
+        if self.nv is not None:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            sm = sorted(m for m, _ in self.samples)
+            reasons = sorted({n for _, rs in self.samples for n in rs})
+            return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(sm), "source": "nvml, 10 ms"}
         if self.p is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.p.terminate()
@@ -143,9 +202,9 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
         mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({self.NAMES[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------------- workloads
