@@ -400,10 +400,12 @@ def run_serve(args, rank, world, local_rank):
     names = {ecl.CC: "cc", ecl.MIS: "mis", ecl.GC: "gc", ecl.MST: "mst", ecl.SCC: "scc"}
     sweep = []
     l0 = ecl.kernel_launches()
-    # warm-up: every code on the largest graph (grows the device memory pool
-    # to its working size once) and on a small one
-    big = max(pool, key=lambda p: p[2])[0]
-    srv.run([(c, gid, 0.0, None) for c in codes for gid in (big, pool[0][0])])
+    # warm-up: a burst of every code on every resident graph at t = 0, so the
+    # slots run concurrently and the stream-ordered memory pool grows to its
+    # concurrent working size before any timed request (growing it later
+    # costs a stall that every in-flight request sees)
+    srv.run([(c, p[0], 0.0, None) for c in codes for p in pool])
+    srv.run([(c, p[0], 0.0, None) for p in sorted(pool, key=lambda p: -p[2])[:8] for c in codes])
     clk = Clocks(local_rank)
     clk.start()
     for rate in (10, 100, 1000, 10000):
