@@ -280,16 +280,29 @@ __global__ void __launch_bounds__(1024) cc_giant(int n, const int* __restrict__ 
       __syncthreads();
     }
   }
-  if (t == 0) {
-    int best = s[0], run = 1, bestrun = 1;
-    for (int i = 1; i < 1024; i++) {
-      run = (s[i] == s[i - 1]) ? run + 1 : 1;
-      if (run > bestrun) {
-        bestrun = run;
-        best = s[i];
-      }
+  // Longest run of equal roots, ties to the smallest root: every run start
+  // finds its end by binary search, then a block-wide max over
+  // (length, ~root) keys (a serial scan by one thread cost ~15 us).
+  unsigned long long key = 0;
+  if (t == 0 || s[t] != s[t - 1]) {
+    int lo = t + 1, hi = 1024;  // first index past the run
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (s[mid] == s[t])
+        lo = mid + 1;
+      else
+        hi = mid;
     }
-    ctr->giant = best;
+    key = ((unsigned long long)(lo - t) << 32) | (0xffffffffu - (unsigned)s[t]);
+  }
+  for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(kFull, key, o));
+  __shared__ unsigned long long wbest[32];
+  if ((t & 31) == 0) wbest[t >> 5] = key;
+  __syncthreads();
+  if (t < 32) {
+    key = wbest[t];
+    for (int o = 16; o > 0; o >>= 1) key = max(key, __shfl_xor_sync(kFull, key, o));
+    if (t == 0) ctr->giant = (int)(0xffffffffu - (unsigned)key);
   }
 }
 
