@@ -43,7 +43,7 @@ void ecl_batch_destroy(ecl_batch* b);
 /* Appends one host graph (copied).  Graphs keep the order they are added in. */
 ecl_status ecl_batch_add(ecl_batch* b, const ecl_graph_view* g);
 
-/* Appends `count` seeded synthetic graphs of the north-star mix: vertex
+/* Appends `count` seeded synthetic graphs of the batched benchmark mix: vertex
  * counts log-uniform in [n_min, n_max], each drawn with equal probability from
  * Erdos-Renyi (average degree 8), a 4-neighbour grid, or R-MAT (edge factor
  * 8, a=.57 b=.19 c=.19), symmetric, weights uniform in [1, weight_max). */

@@ -1,13 +1,13 @@
 """Parity at the benchmark configs' full sizes (one B200).
 
-- CC on the 1024x1024 grid with 5 % of edges deleted, equal to the
+- Grid: CC on the 1024x1024 grid with 5 % of edges deleted, equal to the
   oracle.
-- CC, MIS, GC and MST on symmetrised R-MAT-22 and SCC on the
+- R-MAT-22 suite: CC, MIS, GC and MST on symmetrised R-MAT-22 and SCC on the
   directed R-MAT-22, each equal to the oracle.  The oracles take about 30 s of
   host time here, MST's Kruskal most of it.
-- APSP on ER n=8192.  An O(n^3) host closure would take hours, so
+- APSP: ER n=8192.  An O(n^3) host closure would take hours, so
   32 random rows are checked exactly against Dijkstra from those sources.
-- the batched 4096-graph mix, 16 sampled graphs against the oracle.
+- Batch: the 4096-graph mix, 16 sampled graphs against the oracle.
 """
 import numpy as np
 import pytest
@@ -61,7 +61,7 @@ def test_apsp_er8192_sampled_rows(ecl, orc):
 
 
 def test_batch4096_sampled_graphs(ecl, orc):
-    """the 4096-graph mix (about 1.4 G CSR entries in 3
+    """The 4096-graph mix (about 1.4 G CSR entries in 3
     super-batches), CC+MIS+MST on a CUDA-graph replay; 16 sampled graphs are
     checked against the oracle."""
     b = ecl.Batch()
