@@ -143,9 +143,33 @@ __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restr
   }
 }
 
+// Chunk records of chunk_capacity(m) cover every long row of a CSR whose rows
+// do not overlap (a row of d > kChunk entries needs ceil(d / kChunk) <
+// 2 d / kChunk records).  A malformed CSR with overlapping rows can ask for
+// more: the excess raises ECL_ERR_BAD_GRAPH and is not written.
+constexpr int chunk_capacity(int m) { return 2 * (m / kChunk) + 2; }
+
+__device__ __forceinline__ void cc_push_chunks(int v, int beg, int deg, int2* chunks, int cap, CCCounters* ctr,
+                                               Status* status) {
+  const int nc = (deg + kChunk - 1) / kChunk;
+  const int at = fetch_add(&ctr->nchunks, nc);
+  for (int c = 0; c < nc; c++) {
+    if ((unsigned)(at + c) < (unsigned)cap)
+      chunks[at + c] = make_int2(v, beg + c * kChunk);
+    else
+      raise(status, ECL_ERR_BAD_GRAPH, v);
+  }
+}
+
+// Records the chunk kernels may read: the requested count clamped to cap.
+__device__ __forceinline__ int cc_chunk_total(const CCCounters* ctr, int cap) {
+  const int c = ctr->nchunks;
+  return (c < 0 || c > cap) ? cap : c;
+}
+
 __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ parent,
-                                                int2* __restrict__ chunks, CCCounters* __restrict__ ctr,
+                                                int2* __restrict__ chunks, int chunk_cap, CCCounters* __restrict__ ctr,
                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -156,9 +180,7 @@ __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restr
     if (v < n) cc_row(nindex, v, m, beg, end);
     const int deg = end - beg;
     if (deg > kChunk) {
-      const int nc = (deg + kChunk - 1) / kChunk;
-      const int at = fetch_add(&ctr->nchunks, nc);
-      for (int c = 0; c < nc; c++) chunks[at + c] = make_int2(v, beg + c * kChunk);
+      cc_push_chunks(v, beg, deg, chunks, chunk_cap, ctr, status);
     } else if (deg > 0 && deg <= kLaneMax) {
       int rv = -1;
       for (int i = beg; i < end; i++) {
@@ -193,12 +215,12 @@ __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restr
 
 __global__ void __launch_bounds__(kTPB) cc_chunks(int n, const int* __restrict__ nindex,
                                                   const int* __restrict__ nlist, int* __restrict__ parent,
-                                                  const int2* __restrict__ chunks, const CCCounters* __restrict__ ctr,
-                                                  Status* __restrict__ status) {
+                                                  const int2* __restrict__ chunks, int chunk_cap,
+                                                  const CCCounters* __restrict__ ctr, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = ctr->nchunks;
+  const int total = cc_chunk_total(ctr, chunk_cap);
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
@@ -324,7 +346,8 @@ __device__ __forceinline__ bool cc_rest_wanted(int u, int v, const unsigned char
 __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ parent,
                                                 const unsigned char* __restrict__ ing, int2* __restrict__ chunks,
-                                                CCCounters* __restrict__ ctr, Status* __restrict__ status) {
+                                                int chunk_cap, CCCounters* __restrict__ ctr,
+                                                Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -337,9 +360,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restr
     }
     const int deg = end - beg;
     if (deg > kChunk) {
-      const int nc = (deg + kChunk - 1) / kChunk;
-      const int at = fetch_add(&ctr->nchunks, nc);
-      for (int c = 0; c < nc; c++) chunks[at + c] = make_int2(v, beg + c * kChunk);
+      cc_push_chunks(v, beg, deg, chunks, chunk_cap, ctr, status);
     } else if (deg > 0 && deg <= kLaneMax) {
       int rv = -1;
       for (int i = beg; i < end; i++) {
@@ -374,12 +395,12 @@ __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restr
 __global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ parent,
                                                        const unsigned char* __restrict__ ing,
-                                                       const int2* __restrict__ chunks,
+                                                       const int2* __restrict__ chunks, int chunk_cap,
                                                        const CCCounters* __restrict__ ctr, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = ctr->nchunks;
+  const int total = cc_chunk_total(ctr, chunk_cap);
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
@@ -398,7 +419,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restr
 
 void cc_layout(Carve& c, int n, int m, CCCounters** ctr, int2** chunks, unsigned char** ing = nullptr) {
   *ctr = c.take<CCCounters>(1);
-  *chunks = c.take<int2>((size_t)(2 * (m / kChunk) + 2));
+  *chunks = c.take<int2>((size_t)chunk_capacity(m));
   unsigned char* g = c.take<unsigned char>((size_t)n);
   if (ing) *ing = g;
 }
@@ -435,9 +456,11 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
     ECL_LAUNCH(cc_giant, 1, 1024, 0, stream, g.n, parent, ctr);
     ECL_LAUNCH(cc_mark_giant, grid, kTPB, 0, stream, g.n, parent, ctr, ing);
     mark();
-    ECL_LAUNCH(cc_rest, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, ing, chunks, ctr, status);
+    ECL_LAUNCH(cc_rest, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, ing, chunks, chunk_capacity(g.m), ctr,
+               status);
     mark();
-    ECL_LAUNCH(cc_rest_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, ing, chunks, ctr, status);
+    ECL_LAUNCH(cc_rest_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, ing, chunks, chunk_capacity(g.m), ctr,
+               status);
     mark();
     ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
     mark();
@@ -445,9 +468,11 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   }
   ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
   mark();
-  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, ctr, status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, chunk_capacity(g.m), ctr,
+             status);
   mark();
-  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, chunks, ctr, status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, chunks, chunk_capacity(g.m), ctr,
+             status);
   mark();
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
   mark();
@@ -462,7 +487,13 @@ extern "C" ecl_status ecl_cc(const ecl_graph_view* g, int32_t* label, ecl_opts* 
   if (!opts) opts = &local;
   if (!label) return ECL_ERR_INVALID_ARG;
   Solve s(g, opts);
-  ecl_status st = s.begin(GraphNeeds{}, g ? cc_workspace_bytes(g->nodes, g->edges) : 0);
+  // The sampling path of a graph flagged ECL_GRAPH_SYMMETRIC uses every entry
+  // in both directions, so validation (opts->validate) checks that flag: an
+  // asymmetric graph carrying it would get labels other than the reference's
+  // u < v hooking gives.
+  GraphNeeds needs;
+  needs.symmetric = g && (g->flags & ECL_GRAPH_SYMMETRIC);
+  ecl_status st = s.begin(needs, g ? cc_workspace_bytes(g->nodes, g->edges) : 0);
   if (st != ECL_OK) return s.finish(st);
   int* parent = s.output(label, (size_t)s.n);
   if (!parent) return s.finish(ECL_ERR_OOM);
@@ -489,30 +520,59 @@ namespace ecl {
 namespace {
 
 constexpr size_t kNoAllocBytes = ECL_CC_NOALLOC_SCRATCH_BYTES;
-static_assert(kStatusBytes + sizeof(CCCounters) + 256 + sizeof(int2) * (size_t)(2 * (ECL_CC_NOALLOC_MAX_EDGES / kChunk) + 2) <=
+static_assert(kStatusBytes + sizeof(CCCounters) + 256 + sizeof(int2) * (size_t)chunk_capacity(ECL_CC_NOALLOC_MAX_EDGES) <=
                   kNoAllocBytes,
               "no-alloc scratch too small for ECL_CC_NOALLOC_MAX_EDGES");
 
 static __device__ __align__(256) unsigned char g_cc_noalloc_scratch[kNoAllocBytes];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
+// cuCtxGetCurrent, reached through the runtime's driver entry point so the
+// library needs no link against libcuda.
+typedef int (*CtxGetCurrentFn)(void** ctx);
 
-// Device address of g_cc_noalloc_scratch on the current device, looked up
-// once per device (host code cannot use the symbol itself as a pointer).
+std::mutex g_noalloc_mu;
+struct NoAllocSlot {
+  void* ctx = nullptr;   // context the address belongs to
+  void* addr = nullptr;  // device address of g_cc_noalloc_scratch in it
+};
+NoAllocSlot g_noalloc_slot[64];
+
+// Device address of g_cc_noalloc_scratch on the current device (host code
+// cannot use the symbol itself as a pointer).  It is looked up once per
+// device and kept with the context it was found in: after cudaDeviceReset
+// the device has a new primary context, the module is loaded again, and the
+// address is looked up again instead of reusing a dead one.
 ecl_status noalloc_scratch(int device, void** out) {
   if (device < 0 || device >= 64) return ECL_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[device]) {
+  static CtxGetCurrentFn ctx_get = nullptr;
+  if (!ctx_get) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      set_last_error_msg("ecl_cc_noalloc: cuCtxGetCurrent is not available");
+      return ECL_ERR_CUDA;
+    }
+    ctx_get = reinterpret_cast<CtxGetCurrentFn>(fn);
+  }
+  void* ctx = nullptr;
+  if (ctx_get(&ctx) != 0 || !ctx) {
+    set_last_error_msg("ecl_cc_noalloc: no current CUDA context");
+    return ECL_ERR_CUDA;
+  }
+  NoAllocSlot& slot = g_noalloc_slot[device];
+  if (slot.ctx != ctx || !slot.addr) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_cc_noalloc_scratch);
     if (e != cudaSuccess) {
       set_last_error("cudaGetSymbolAddress(g_cc_noalloc_scratch)", e);
       return ECL_ERR_CUDA;
     }
-    g_noalloc_addr[device] = p;
+    slot.ctx = ctx;
+    slot.addr = p;
   }
-  *out = g_noalloc_addr[device];
+  *out = slot.addr;
   return ECL_OK;
 }
 
@@ -545,8 +605,10 @@ extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t
   ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
   const int grid = dev.grid_blocks(kTPB);
   ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
-  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, ctr, status);
-  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, ctr, status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, chunk_capacity(edges), ctr,
+             status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, chunk_capacity(edges), ctr,
+             status);
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, nodes, label);
   Status hs{};
   ECL_CUDA_TRY(cudaMemcpyAsync(&hs, status, sizeof(hs), cudaMemcpyDeviceToHost, stream));

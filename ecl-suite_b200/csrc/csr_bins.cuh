@@ -18,12 +18,25 @@ namespace dev {
 constexpr int kBinLane = 32;
 constexpr int kBinChunk = 256;
 
+// Chunk records of the long rows.  `cap` records fit: 2 * (m / chunk) + 2
+// covers every row of a CSR whose rows do not overlap (each long row of d
+// entries needs ceil(d / chunk) < 2 d / chunk records); a malformed CSR whose
+// rows overlap can ask for more, and the excess is reported, not written.
 struct RowChunks {
   int2* rec;   // (vertex, first entry of the chunk)
-  int* count;  // number of records
+  int* count;  // records requested (may exceed cap on a malformed CSR)
+  int cap;     // records the buffer holds
 };
 
-inline size_t row_chunk_capacity(int m) { return 2 * (size_t)(m / kBinChunk) + 2; }
+__host__ __device__ constexpr size_t row_chunk_capacity(int m, int chunk = kBinChunk) {
+  return 2 * (size_t)(m / chunk) + 2;
+}
+
+// Records a consumer may read: the requested count clamped to the capacity.
+__device__ __forceinline__ int chunk_total(const RowChunks& rc) {
+  const int c = *rc.count;
+  return (c < 0 || c > rc.cap) ? rc.cap : c;
+}
 
 // Row [beg, end) of v; a malformed row reports ECL_ERR_BAD_GRAPH and is empty.
 __device__ __forceinline__ void csr_row(const int* nindex, int v, int m, int& beg, int& end, Status* status) {
@@ -39,9 +52,12 @@ __device__ __forceinline__ void csr_row(const int* nindex, int v, int m, int& be
 // warp calls; lanes with `is_long` cut [beg, end) into kChunkLen-entry
 // records (vertex, first entry).  One atomic per warp reserves all of them
 // (R-MAT-22 has ~50k rows over 256 entries; an atomic per row on one counter
-// would serialise in L2); the records land in lane order.
+// would serialise in L2); the records land in lane order.  Records past the
+// capacity (only a CSR with overlapping rows asks for them) raise
+// ECL_ERR_BAD_GRAPH and are dropped.
 template <int kChunkLen>
-__device__ __forceinline__ void push_chunks_warp(int2* rec, int* count, bool is_long, int v, int beg, int end) {
+__device__ __forceinline__ void push_chunks_warp(const RowChunks& rc, bool is_long, int v, int beg, int end,
+                                                 Status* status) {
   const int lane = threadIdx.x & 31;
   const int nc = is_long ? (end - beg + kChunkLen - 1) / kChunkLen : 0;
   if (!__any_sync(kFull, nc > 0)) return;
@@ -53,9 +69,14 @@ __device__ __forceinline__ void push_chunks_warp(int2* rec, int* count, bool is_
   }
   const int total = __shfl_sync(kFull, incl, 31);
   int base = 0;
-  if (lane == 0) base = fetch_add(count, total);
+  if (lane == 0) base = fetch_add(rc.count, total);
   base = __shfl_sync(kFull, base, 0) + incl - nc;
-  for (int c = 0; c < nc; c++) rec[base + c] = make_int2(v, beg + c * kChunkLen);
+  for (int c = 0; c < nc; c++) {
+    if ((unsigned)(base + c) < (unsigned)rc.cap)  // a wrapped counter stays out too
+      rc.rec[base + c] = make_int2(v, beg + c * kChunkLen);
+    else
+      raise(status, ECL_ERR_BAD_GRAPH, v);
+  }
 }
 
 // Warp-aggregated slot in an append-only list; every lane of the warp calls.

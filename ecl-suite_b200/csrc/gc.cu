@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
     const int dv = end - beg;
     const unsigned hv = (v < n) ? gc_h(vhash, v) : 0u;
     int h = 0;
-    push_chunks_warp<kBinChunk>(rc.rec, rc.count, dv > kBinChunk, v, beg, end);
+    push_chunks_warp<kBinChunk>(rc, dv > kBinChunk, v, beg, end, status);
     if (v < n && dv <= kBinLane) {
       for (int i0 = beg; i0 < end; i0 += kInitBatch) {
         int u[kInitBatch], cls[kInitBatch];
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = *rc.count;
+  const int total = chunk_total(rc);
   for (int c = warp; c < total; c += nwarps) {
     const int2 r = rc.rec[c];
     const int v = r.x;
@@ -498,7 +498,7 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
-  const RowChunks rc{b.chunks, &b.ctl->nchunks};
+  const RowChunks rc{b.chunks, &b.ctl->nchunks, (int)row_chunk_capacity(g.m)};
   // key bits that vary: 32 hash bits + enough bits for any degree <= m
   int degbits = 1;
   while (degbits < 31 && ((long long)1 << degbits) <= (long long)g.m) degbits++;

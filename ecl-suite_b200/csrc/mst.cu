@@ -260,7 +260,8 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
     int rv = v;
     if (!kLight && deg > 0 && v < n) rv = ld(&parent[v]);
     if (kLight)  // chunk records are built once, in the light pass
-      push_chunks_warp<kChunk>(chunks, &ctl->nchunks, deg > kChunk, v, beg, end);
+      push_chunks_warp<kChunk>(RowChunks{chunks, &ctl->nchunks, (int)row_chunk_capacity(m, kChunk)}, deg > kChunk, v,
+                               beg, end, status);
     // lane level: all lanes step through offset k together
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch)
@@ -290,13 +291,14 @@ template <bool kLight>
 __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict__ nindex, const int* __restrict__ nlist,
                                                    const int* __restrict__ eweight, int* __restrict__ parent,
                                                    int4* __restrict__ wl, int cap, MSTCtl* __restrict__ ctl,
-                                                   const int2* __restrict__ chunks, Status* __restrict__ status) {
+                                                   const int2* __restrict__ chunks, int chunk_cap,
+                                                   Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   const int thr = ctl->threshold;
   int* cnt = &ctl->wlcount[kLight ? 0 : 1][0];
-  const int total = ctl->nchunks;
+  const int total = min((unsigned)ctl->nchunks, (unsigned)chunk_cap);
   __shared__ int4 stage_buf[kTPB / 32][kStage];
   Stage stg{stage_buf[threadIdx.x >> 5]};
   bool overflow = false;
@@ -461,6 +463,7 @@ struct MSTBufs {
   int* parent;
   u64* minv;
   int2* chunks;
+  int chunk_cap;
   int4* wlA;
   int4* wlB;
   int cap;
@@ -470,7 +473,8 @@ void mst_layout(Carve& c, int n, int m, bool symmetric, MSTBufs* b) {
   b->ctl = c.take<MSTCtl>(1);
   b->parent = c.take<int>((size_t)n);
   b->minv = c.take<u64>((size_t)2 * n);
-  b->chunks = c.take<int2>((size_t)(2 * (m / kChunk) + 2));
+  b->chunks = c.take<int2>(row_chunk_capacity(m, kChunk));
+  b->chunk_cap = (int)row_chunk_capacity(m, kChunk);
   // v<n entries: at most m/2 in a symmetric, self-loop-free graph, else m.
   b->cap = symmetric ? m / 2 + 1 : (m > 0 ? m : 1);
   b->wlA = c.take<int4>((size_t)b->cap);
@@ -510,13 +514,13 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
         ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, status);
         ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, status);
+                   b.ctl, b.chunks, b.chunk_cap, status);
       } else {
         ECL_LAUNCH(mst_flatten, grid, kTPB, 0, stream, g.n, b.parent);
         ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, status);
         ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, status);
+                   b.ctl, b.chunks, b.chunk_cap, status);
       }
       mark();
       ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.cap, b.parent,

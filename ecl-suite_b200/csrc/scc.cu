@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       io[v] = io_pack(v, v);
     }
     const int deg = end - beg;
-    push_chunks_warp<kBinChunk>(rc.rec, rc.count, deg > kBinChunk, v, beg, end);
+    push_chunks_warp<kBinChunk>(rc, deg > kBinChunk, v, beg, end, status);
     bool out = false;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = *rc.count;
+  const int total = chunk_total(rc);
   for (int c = warp; c < total; c += nwarps) {
     const int2 r = rc.rec[c];
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
@@ -247,7 +247,7 @@ __global__ void __launch_bounds__(kTPB) scc_build_chunks(int n, const int* __res
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = *rc.count;
+  const int total = chunk_total(rc);
   for (int c = warp; c < total; c += nwarps) {
     const int2 r = rc.rec[c];
     const bool live = scc_live(flags, r.x);
@@ -421,7 +421,7 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
     return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.flags, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
-  const RowChunks rc{b.chunks, b.nchunks};
+  const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m)};
   ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.io, rc, status);
   ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, rc, status);
   mark();

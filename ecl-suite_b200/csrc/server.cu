@@ -84,12 +84,9 @@ size_t request_bytes(int code, const GraphDev& g) {
   return align256(kStatusBytes) + align256(ws_bytes(code, g)) + align256(out_bytes(code, g));
 }
 
-// Launches request r on slot s.  Memory layout: status | workspace | output.
-ecl_status launch(ecl_server* sv, Slot& s, ecl_request& r) {
+// Everything request r puts on slot s's stream after its memory is allocated.
+ecl_status enqueue_request(ecl_server* sv, Slot& s, ecl_request& r) {
   const GraphDev& g = sv->graphs[(size_t)r.graph].g;
-  const size_t need = request_bytes(r.code, g);
-  ECL_CUDA_TRY(cudaMallocAsync(&s.mem, need, s.stream));
-  s.bytes = need;
   char* base = static_cast<char*>(s.mem);
   dev::Status* status = reinterpret_cast<dev::Status*>(base);
   char* ws = base + align256(kStatusBytes);
@@ -111,7 +108,25 @@ ecl_status launch(ecl_server* sv, Slot& s, ecl_request& r) {
   if (r.out) ECL_CUDA_TRY(cudaMemcpyAsync(r.out, out, out_bytes(r.code, g), cudaMemcpyDeviceToHost, s.stream));
   if (total_dev) ECL_CUDA_TRY(cudaMemcpyAsync(s.htotal, total_dev, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s.stream));
   ECL_CUDA_TRY(cudaMemcpyAsync(s.hstatus, status, sizeof(dev::Status), cudaMemcpyDeviceToHost, s.stream));
-  ECL_CUDA_TRY(cudaFreeAsync(s.mem, s.stream));
+  return ECL_OK;
+}
+
+// Launches request r on slot s.  Memory layout: status | workspace | output.
+// The request's memory goes back to the pool on the slot's stream whether or
+// not every step was enqueued, so a failed launch leaks nothing.
+ecl_status launch(ecl_server* sv, Slot& s, ecl_request& r) {
+  const GraphDev& g = sv->graphs[(size_t)r.graph].g;
+  const size_t need = request_bytes(r.code, g);
+  ECL_CUDA_TRY(cudaMallocAsync(&s.mem, need, s.stream));
+  s.bytes = need;
+  const ecl_status st = enqueue_request(sv, s, r);
+  const cudaError_t fe = cudaFreeAsync(s.mem, s.stream);
+  s.mem = nullptr;
+  if (st != ECL_OK) return st;
+  if (fe != cudaSuccess) {
+    set_last_error("cudaFreeAsync", fe);
+    return ECL_ERR_CUDA;
+  }
   ECL_CUDA_TRY(cudaEventRecord(s.done, s.stream));
   return ECL_OK;
 }

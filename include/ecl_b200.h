@@ -175,8 +175,12 @@ ecl_status ecl_apsp(const ecl_graph_view* g, int32_t* dist, int64_t ld, ecl_opts
  *  - Graphs with more than ECL_CC_NOALLOC_MAX_EDGES CSR entries are rejected
  *    with ECL_ERR_UNSUPPORTED (use ecl_cc for those).
  *  - The first call on each device looks up the array's device address
- *    (cudaGetSymbolAddress) with that device current; make that first call
- *    before any stream capture.
+ *    (cudaGetSymbolAddress) with that device current, and looks it up again
+ *    after the device's context was replaced (cudaDeviceReset).
+ *  - Do not call it while its stream is being captured into a CUDA graph
+ *    (nor while a global or relaxed-mode capture is active on another
+ *    stream): every call copies the status back and synchronises the stream,
+ *    which a capture does not allow.
  *  - All calls share the one array and it keeps the last call's contents (the
  *    call clears what must start at zero).  Calls that overlap on the GPU --
  *    different streams, or threads calling at once -- race on it; serialise

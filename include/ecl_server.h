@@ -36,7 +36,11 @@ typedef struct ecl_request {
   int32_t code;        /* ecl_code: ECL_CC, ECL_MIS, ECL_GC, ECL_MST or ECL_SCC */
   int32_t graph;       /* id from ecl_server_add_graph */
   double arrival_s;    /* arrival time, seconds after the start of the run */
-  void* out;           /* host buffer for the result (the code's single-graph layout), or NULL */
+  void* out;           /* host buffer for the result (the code's single-graph layout), or NULL.
+                          It must be page-locked (cudaHostAlloc / cudaHostRegister): the result is
+                          copied back asynchronously on the request's slot stream, and a pageable
+                          buffer would make that copy wait for the solve, stalling the one host
+                          thread that admits and completes every slot. */
   /* filled in by ecl_server_run: */
   uint64_t total_weight; /* MST only */
   double latency_s;      /* completion - arrival */

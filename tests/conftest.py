@@ -80,3 +80,17 @@ def undirected(n, pairs, weights=None):
     e = [e[i] for i in order]
     w = [w[i] for i in order] if weights is not None else None
     return from_edges(n, e, w, symmetric=True)
+
+
+def overlapping_rows(n=63, m=4096, seed=7):
+    """A CSR whose rows overlap: every even row is [0, m) and every odd row is
+    [m, 0).  The odd rows are malformed (end < beg); the even rows together ask
+    for far more long-row chunk records than a CSR of m entries can need.  Every
+    entry is a valid vertex id, so nothing reads outside the arrays."""
+    import ecl_b200
+
+    rng = np.random.default_rng(seed)
+    nindex = np.array([0 if v % 2 == 0 else m for v in range(n + 1)], np.int32)
+    nlist = rng.integers(0, n, size=m).astype(np.int32)
+    w = rng.integers(1, 1000, size=m).astype(np.int32)
+    return ecl_b200.Graph(nindex, nlist, w, symmetric=True)

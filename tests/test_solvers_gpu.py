@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from conftest import from_edges, undirected
+from conftest import from_edges, overlapping_rows, undirected
 
 pytestmark = pytest.mark.gpu
 
@@ -193,3 +193,65 @@ def test_apsp_reference_padded_layout(ecl, orc):
     assert st == 0
     assert np.array_equal(out[:100, :100], orc.apsp(g))
     assert np.all(out[100:, :] == ecl.APSP_INF) and np.all(out[:, 100:] == ecl.APSP_INF)
+
+
+# ---------------------------------------------------------- malformed input and wait limits
+
+
+@pytest.mark.parametrize("code", ["cc", "mis", "gc", "mst", "scc"])
+def test_overlapping_rows_are_rejected_on_the_device(ecl, orc, code):
+    """Without host validation the kernels see the overlapping rows: each code
+    reports ECL_ERR_BAD_GRAPH (chunk records beyond the buffer are counted,
+    not written), and the next solve on the same device is correct."""
+    g = overlapping_rows()
+    with pytest.raises(ecl.EclError) as e:
+        getattr(ecl, code)(g.to_device(), validate=False)
+    assert e.value.status == ecl.ERR_BAD_GRAPH
+    ok = ecl.gen_rmat(12, 8, seed=2, weight_seed=3)
+    assert np.array_equal(ecl.cc(ok), orc.cc(ok))
+
+
+def test_mis_wait_limit_reports_no_convergence_then_recovers(ecl, orc):
+    """A 100k-vertex path needs many dependent sweeps; capped at max_rounds = 1
+    the persistent launch gives up with ECL_ERR_NO_CONVERGENCE instead of
+    sweeping on, and the next solve on the same stream is bit-exact."""
+    import torch
+
+    n = 100000
+    g = undirected(n, [(i, i + 1) for i in range(n - 1)])
+    dg = g.to_device()
+    with pytest.raises(ecl.EclError) as e:
+        ecl.mis(dg, max_rounds=1)
+    assert e.value.status == ecl.ERR_NO_CONVERGENCE
+    torch.cuda.synchronize()
+    assert np.array_equal(ecl.mis(dg).cpu().numpy(), orc.mis(g))
+
+
+def test_scc_round_limit_reports_no_convergence_then_recovers(ecl, orc):
+    """A chain of 2-cycles c0 -> c1 -> ... needs one trimming round per cycle
+    (only the last cycle's maximum reaches back); max_rounds = 1 stops after
+    the first round with ECL_ERR_NO_CONVERGENCE, and the next solve on the
+    same stream equals the oracle."""
+    k = 64
+    edges = []
+    for c in range(k):
+        a, b = 2 * c, 2 * c + 1
+        edges += [(a, b), (b, a)]
+        if c + 1 < k:
+            edges.append((b, 2 * c + 2))
+    g = from_edges(2 * k, sorted(edges))
+    dg = g.to_device()
+    with pytest.raises(ecl.EclError) as e:
+        ecl.scc(dg, max_rounds=1)
+    assert e.value.status == ecl.ERR_NO_CONVERGENCE
+    assert np.array_equal(ecl.scc(dg).cpu().numpy(), orc.scc(g))
+
+
+def test_cc_validate_checks_the_symmetric_flag(ecl):
+    """CC's sampling path uses each entry in both directions, so with
+    validation on, an asymmetric graph flagged symmetric is rejected on the
+    host before any launch."""
+    g = from_edges(4, [(0, 1), (2, 3), (3, 2)], symmetric=True)
+    with pytest.raises(ecl.EclError) as e:
+        ecl.cc(g, validate=True)
+    assert e.value.status == ecl.ERR_BAD_GRAPH

@@ -10,7 +10,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import undirected
+from conftest import overlapping_rows, undirected
 
 pytestmark = pytest.mark.gpu
 
@@ -54,3 +54,22 @@ def test_cc_noalloc_rejects_graphs_beyond_its_limit(ecl):
     st = f(1, limit + 1, small.data_ptr(), small.data_ptr(), small.data_ptr(), None)
     assert st == ecl.ERR_UNSUPPORTED
     assert b"ECL_CC_NOALLOC_MAX_EDGES" in ecl.lib.ecl_last_error()
+
+
+def test_cc_noalloc_overlapping_rows_stay_inside_the_array(ecl, orc):
+    """A CSR whose rows overlap asks for more long-row chunk records than the
+    fixed array holds for its edge count: the call reports ECL_ERR_BAD_GRAPH
+    and writes nothing past its records, and the next call is still exact."""
+    import torch
+
+    f = _entry(ecl)
+    stream = torch.cuda.current_stream().cuda_stream
+    g = overlapping_rows()
+    dg = g.to_device()
+    out = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
+    assert f(g.nodes, g.edges, dg.nindex.data_ptr(), dg.nlist.data_ptr(), out.data_ptr(), stream) == ecl.ERR_BAD_GRAPH
+    ok = ecl.gen_rmat(13, 16, seed=2)
+    dok = ok.to_device()
+    out = torch.empty(ok.nodes, dtype=torch.int32, device="cuda")
+    assert f(ok.nodes, ok.edges, dok.nindex.data_ptr(), dok.nlist.data_ptr(), out.data_ptr(), stream) == ecl.OK
+    assert np.array_equal(out.cpu().numpy(), orc.cc(ok))
