@@ -76,7 +76,7 @@ def job_rate(units_per_rank, world, max_seconds):
     return world * units_per_rank / max_seconds
 
 
-def parse():
+def parse(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
@@ -87,7 +87,11 @@ def parse():
     p.add_argument("--batch-count", type=int, default=4096)
     p.add_argument("--scale", type=int, default=22)
     p.add_argument("--e2e-steps", type=int, default=2)
-    return p.parse_args()
+    p.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false",
+                   help="skip the CPU baseline leg of our arm")
+    p.add_argument("--no-other-configs", dest="other_configs", action="store_false",
+                   help="suite only: skip the grid, APSP, batched and served configs measured after it")
+    return p.parse_args(argv)
 
 
 def peaks():
@@ -210,9 +214,11 @@ class Clocks:
 # ---------------------------------------------------------------- workloads
 
 
-def make_suite_graphs(ecl, scale):
-    sym = ecl.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=True, weight_seed=3, weight_max=1 << 20)
-    dirg = ecl.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=False)
+def make_suite_graphs(gen, scale):
+    """The suite's graphs from `gen`: the product library in our arm, the
+    oracle's restated generators (same bytes) in the reference arm."""
+    sym = gen.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=True, weight_seed=3, weight_max=1 << 20)
+    dirg = gen.gen_rmat(scale, 16, 0.57, 0.19, 0.19, seed=2, symmetrise=False)
     return sym, dirg
 
 
@@ -236,7 +242,8 @@ def phase_bytes(code, phase, n, m):
         ("mis", 2): 2 * n,
         ("gc", 0): csr + 4 * (m // 2) + 4 * n,     # init: CSR read, higher-priority half of nl2 + counts written
         ("gc", 1): 7 * 24 * n,                     # keys + 7 radix passes over (8 B key, 4 B value), read + write
-        ("gc", 2): 4 * (n + 1) + 4 * (m // 2) + 12 * n,  # pull: higher-priority half read once, order, colours
+        ("gc", 2): None,                           # core: latency-bound, no byte model (its entries are booked to pull)
+        ("gc", 3): 4 * (n + 1) + 4 * (m // 2) + 12 * n,  # pull: higher-priority half read once, order, colours
         ("mst", 0): 16 * n,
         ("mst", 1): 4 * (n + 1) + 8 * m,           # light scan: CSR + weights
         ("mst", 2): 16 * n,
@@ -246,14 +253,14 @@ def phase_bytes(code, phase, n, m):
         ("scc", 1): csr + 4 * n,
         ("scc", 2): 8 * m + 12 * n,
     }
-    return table.get((code, phase), csr)
+    return table[(code, phase)] if (code, phase) in table else csr
 
 
 PHASE_NAMES = {
     "cc": ["cc_init", "cc_hook", "cc_chunks", "cc_flatten"],
     "cc_sym": ["cc_init+sample+giant", "cc_rest", "cc_rest_chunks", "cc_flatten"],
     "mis": ["mis_init", "mis_run", "mis_emit"],
-    "gc": ["gc_init+chunks", "gc_keys+radix_sort", "gc_pull"],
+    "gc": ["gc_init+chunks", "gc_keys+radix_sort", "gc_core", "gc_pull"],
     "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
             "mst_boruvka(heavy)"],
     "scc": ["scc_mark+chunks", "scc_build+chunks", "scc_solve"],
@@ -269,7 +276,7 @@ def phase_code(code, g):
 # ---------------------------------------------------------------- our arm
 
 
-def run_batch(args, rank, world, local_rank):
+def bench_batch(args, rank, world, local_rank):
     """Batched config: 4096 graphs (n log-uniform in [1k, 200k], seed 5;
     ER d=8 / grid / R-MAT ef=8; weights in [1, 2^16)), CC+MIS+MST per graph.
     value = graphs/s of the batched engine (one CUDA-graph replay per step);
@@ -356,15 +363,16 @@ def run_batch(args, rank, world, local_rank):
                    "codes": "CC+MIS+MST", "parallelism": f"replicas x{world}"},
         "plain_graphs_per_s": plain_gps, "plain_ms": plain_ms, "speedup_vs_plain": value / plain_gps,
         "edges_per_s": 3 * tot_m * args.steps / (ms / 1e3),
-        "cuda_graph_replay": replay, "tuned": {"blocks_per_sm": tuned[0], "mst_light_factor": tuned[1]},
+        "cuda_graph_replay": replay, "tuned": tuned.as_dict(),
         "setup_s": {"generate": round(gen_s, 2), "build_upload": round(build_s, 2), "tune": round(tune_s, 2)},
         "gpu_launches": int(launches), "clocks": clocks,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    del dgs, ws, o_cc, o_mis, o_mst
+    b.close()
+    return line
 
 
-def run_serve(args, rank, world, local_rank):
+def bench_serve(args, rank, world, local_rank):
     """Served config: Poisson arrivals (seed 6) of CC/MIS/GC/MST/SCC requests
     on a pool of resident seeded graphs (R-MAT or grid, n log-uniform in
     [10k, 8M], edge factor 8-16, weights uniform in [1, 2^20)), admitted
@@ -451,20 +459,15 @@ def run_serve(args, rank, world, local_rank):
         "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": sweep, "setup_s": round(setup_s, 2),
         "gpu_launches": int(ecl.kernel_launches() - l0), "clocks": clocks,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    srv.close()
+    return line
 
 
-def run_ours(args, rank, world, local_rank):
+def bench_plain(args, rank, world, local_rank):
     import numpy as np
     import torch
 
     import ecl_b200 as ecl
-
-    if args.workload == "batch":
-        return run_batch(args, rank, world, local_rank)
-    if args.workload == "serve":
-        return run_serve(args, rank, world, local_rank)
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -474,16 +477,15 @@ def run_ours(args, rank, world, local_rank):
     if args.workload == "suite":
         sym, dirg = make_suite_graphs(ecl, args.scale)
         jobs = [(c, sym) for c in CODES_SYM] + [("scc", dirg)]
-        wl_name = (f"rmat{args.scale}-suite: CC+MIS+GC+MST on symmetrised R-MAT-{args.scale} "
-                   f"(n={sym.nodes}, m={sym.edges}), SCC on directed R-MAT-{args.scale} (m={dirg.edges})")
+        wl_name = suite_name(args.scale, sym, dirg)
     elif args.workload == "grid":
         g = grid_graph(ecl)
         jobs = [("cc", g)]
-        wl_name = f"grid1024-cc: CC on 1024x1024 grid, 5% deleted (n={g.nodes}, m={g.edges})"
+        wl_name = grid_name(g)
     else:
         g = apsp_graph(ecl)
         jobs = [("apsp", g)]
-        wl_name = f"er8192-apsp: blocked FW on ER n=8192 p=0.001 (m={g.edges})"
+        wl_name = apsp_name(g)
 
     dgs = {}
     for code, g in jobs:
@@ -562,7 +564,9 @@ def run_ours(args, rank, world, local_rank):
     ms_per_step = total_ms / args.steps
 
     # dominant kernel phase and its roofline
-    dom = max(phase_tot.items(), key=lambda kv: kv[1]) if phase_tot else None
+    # the dominant phase among those with a byte model
+    modelled = {k: v for k, v in phase_tot.items() if k[0] == "apsp" or phase_bytes(k[0], k[1], 1, 1) is not None}
+    dom = max(modelled.items(), key=lambda kv: kv[1]) if modelled else None
     pk = peaks()
     roof = None
     if dom is not None and jobs[0][0] != "apsp":
@@ -651,13 +655,13 @@ def run_ours(args, rank, world, local_rank):
                "ms_per_step": e_ms / args.e2e_steps}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_baseline:
         if args.workload == "suite":
-            cpu = cpu_baseline(ecl, scale=min(args.scale, 21))
+            cpu = cpu_baseline(sym, dirg)
         elif args.workload == "grid":
-            cpu = cpu_baseline_grid(ecl)
+            cpu = cpu_baseline_grid(g)
         else:
-            cpu = cpu_baseline_apsp(ecl)
+            cpu = cpu_baseline_apsp()
 
     per_code = {c: {"edges": g.edges, "ms": per_code_ms[c] / args.steps,
                     "edges_per_s": g.edges / (per_code_ms[c] / args.steps / 1e3),
@@ -670,20 +674,62 @@ def run_ours(args, rank, world, local_rank):
         "value": value, "unit": unit, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic (seeded generators: R-MAT / grid / Erdos-Renyi)",
-        "config": {"workload": wl_name, "l2": "256 MiB write (> 126 MB L2) before every solve",
-                   "parallelism": f"replicas x{world}"},
+        "config": {"workload": wl_name, "l2": L2_NOTE}, "parallelism": f"replicas x{world}",
         "per_code": per_code, "phase_ms": phases, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
+    del dgs, ws, outs, flush
+    return line
+
+
+def other_configs(args, local_rank):
+    """The other four configs, measured after the headline suite on the same
+    GPU (1 GPU only): the 1024x1024 grid CC, APSP on ER n=8192, the batched
+    4096-graph mix and the served Poisson stream.  Each has its own clocks;
+    none is inside the headline's timed region."""
+    import torch
+
+    out = {}
+    plan = [("grid", dict(workload="grid", steps=args.steps, warmup=args.warmup, e2e_steps=args.e2e_steps)),
+            ("apsp", dict(workload="apsp", steps=min(args.steps, 5), warmup=min(args.warmup, 3),
+                          e2e_steps=min(args.e2e_steps, 1))),
+            ("batch", dict(workload="batch", steps=min(args.steps, 5), warmup=min(args.warmup, 3))),
+            ("serve", dict(workload="serve"))]
+    for name, over in plan:
+        sub = argparse.Namespace(**vars(args))
+        for k, v in over.items():
+            setattr(sub, k, v)
+        t0 = time.perf_counter()
+        try:
+            if name == "batch":
+                r = bench_batch(sub, 0, 1, local_rank)
+            elif name == "serve":
+                r = bench_serve(sub, 0, 1, local_rank)
+            else:
+                r = bench_plain(sub, 0, 1, local_rank)
+        except Exception as ex:  # reported in the line; the headline stands on its own
+            r = {"error": f"{type(ex).__name__}: {ex}"}
+        r["wall_s"] = round(time.perf_counter() - t0, 1)
+        out[name] = r
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        print(f"bench: {name} done in {r['wall_s']} s", file=sys.stderr, flush=True)
+    return out
 
 
 # ---------------------------------------------------------------- CPU baseline / reference arm
+#
+# Both use the checker code under oracle/ only: the reference's own CPU
+# routines and CUDA build compiled from its sources (oracle/_ref), the C
+# restatement (oracle/_build) for the codes the reference has no CPU solver
+# for, and the restated generators, so the reference arm never loads the
+# product library.
 
 
 def _orc():
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    p = os.path.join(ROOT, "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
     import oracle
 
     return oracle
@@ -713,6 +759,7 @@ def _ref():
 # this machine is the baseline.  MST is the reference's own serial cpuMST
 # (ECL-MST_10-atomic.cu:112) when oracle/_ref is built.
 _CPU_PICK = {}
+SUITE_LEGS = ("cc", "mis", "gc", "mst", "scc")
 
 
 def cpu_leg(orc, code, g):
@@ -734,53 +781,85 @@ def cpu_leg(orc, code, g):
     return dt, "port (serial)", 1
 
 
-def cpu_suite_once(ecl, sym, dirg, orc, ref):
-    """One pass of the CPU suite.  Returns (edges, seconds, kinds, cores)."""
+def suite_leg(orc, ref, code, sym, dirg):
+    """One code of the CPU suite: returns (edges, seconds, kind, cores)."""
     import numpy as np
 
-    t_total, e_total, kinds, cores = 0.0, 0, {}, {}
-    for code in ("cc", "mis", "gc"):
-        dt, kinds[code], cores[code] = cpu_leg(orc, code, sym)
-        t_total += dt
-        e_total += sym.edges
-    out = np.zeros(sym.edges, np.uint8)
+    if code == "scc":
+        dt, kind, cores = cpu_leg(orc, "scc", dirg)
+        return dirg.edges, dt, kind, cores
+    if code != "mst":
+        dt, kind, cores = cpu_leg(orc, code, sym)
+        return sym.edges, dt, kind, cores
+    out = np.zeros(max(sym.edges, 1), np.uint8)
     t0 = time.perf_counter()
     if ref is not None:
         P = lambda a: C.c_void_p(a.ctypes.data)
         ref.eclref_mst_cpu(sym.nodes, sym.edges, P(sym.nindex), P(sym.nlist), P(sym.eweight), P(out))
-        kinds["mst"] = "reference"
+        kind = "reference"
     else:
         orc.mst(sym)
-        kinds["mst"] = "port"
-    cores["mst"] = 1
-    t_total += time.perf_counter() - t0
-    e_total += sym.edges
-    dt, kinds["scc"], cores["scc"] = cpu_leg(orc, "scc", dirg)
-    t_total += dt
-    e_total += dirg.edges
-    return e_total, t_total, kinds, cores
+        kind = "port (serial)"
+    return sym.edges, time.perf_counter() - t0, kind, 1
 
 
-def cpu_baseline(ecl, scale):
-    orc = _orc()
-    ref = _ref()
-    sym, dirg = make_suite_graphs(ecl, scale)
-    e, t, kinds, cores = cpu_suite_once(ecl, sym, dirg, orc, ref)
-    return {"value": e / t, "unit": "edges/s", "cores": max(cores.values()),
-            "kind": "reference" if kinds.get("mst") == "reference" else "port",
-            "sample": f"one pass of the suite on R-MAT-{scale} (same generator parameters): CC/MIS/GC/SCC by the "
-                      f"faster of the serial C oracle and its OpenMP rendering ({orc.omp_threads()} threads) on this "
-                      f"host, MST by the reference's own serial cpuMST; {t:.1f} s",
-            "per_code_kind": kinds, "per_code_cores": cores}
+def overall_kind(kinds):
+    """'reference' or 'port' when every code agrees, else 'mixed' (the
+    per-code kinds are reported beside it)."""
+    ks = {("reference" if k == "reference" else "port") for k in kinds.values()}
+    return ks.pop() if len(ks) == 1 else "mixed"
 
 
-def grid_graph(ecl):
-    return ecl.gen_grid(1024, 1024, 0.05, seed=1)
+def suite_rate(times, edges):
+    """Suite edges/s from per-code mean times: sum of one pass's edges over the
+    sum of the codes' mean solve times."""
+    codes = [c for c in SUITE_LEGS if times.get(c)]
+    t = sum(sum(times[c]) / len(times[c]) for c in codes)
+    return sum(edges[c] for c in codes) / t
 
 
-def apsp_graph(ecl, n=8192):
+def cpu_baseline(sym, dirg):
+    """One pass of the CPU suite on the bench's own R-MAT graphs."""
+    orc, ref = _orc(), _ref()
+    kinds, cores, times, edges = {}, {}, {}, {}
+    for code in SUITE_LEGS:
+        edges[code], dt, kinds[code], cores[code] = suite_leg(orc, ref, code, sym, dirg)
+        times[code] = [dt]
+    tot = sum(t[0] for t in times.values())
+    return {"value": suite_rate(times, edges), "unit": "edges/s", "cores": max(cores.values()),
+            "kind": overall_kind(kinds),
+            "sample": f"one pass of the suite on the same graphs: MST by the reference's own serial cpuMST, "
+                      f"CC/MIS/GC/SCC (no CPU solver in the reference) by the faster of the serial C oracle and "
+                      f"its OpenMP rendering ({orc.omp_threads()} threads) on this host; {tot:.1f} s",
+            "per_code_kind": kinds, "per_code_cores": cores,
+            "per_code_s": {c: round(times[c][0], 3) for c in SUITE_LEGS}}
+
+
+def grid_graph(gen):
+    return gen.gen_grid(1024, 1024, 0.05, seed=1)
+
+
+def apsp_graph(gen, n=8192):
     # ER with the same expected degree as n=8192, p=0.001 (about 8.2)
-    return ecl.gen_er(n, 0.001 * 8192 / n, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+    return gen.gen_er(n, 0.001 * 8192 / n, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+
+
+def suite_name(scale, sym, dirg):
+    return (f"rmat{scale}-suite: CC+MIS+GC+MST on symmetrised R-MAT-{scale} "
+            f"(n={sym.nodes}, m={sym.edges}), SCC on directed R-MAT-{scale} (m={dirg.edges})")
+
+
+def grid_name(g):
+    return f"grid1024-cc: CC on 1024x1024 grid, 5% deleted (n={g.nodes}, m={g.edges})"
+
+
+def apsp_name(g):
+    return f"er8192-apsp: blocked FW on ER n=8192 p=0.001 (m={g.edges})"
+
+
+# the timed region of either arm runs on inputs larger than L2 (the suite) or
+# after a flush; the CPU arm's inputs exceed every host cache
+L2_NOTE = "256 MiB write (> 126 MB L2) before every GPU solve; CPU legs run on the same host arrays"
 
 
 def cpu_grid_once(g, orc):
@@ -788,9 +867,8 @@ def cpu_grid_once(g, orc):
     return g.edges, dt, cores
 
 
-def cpu_baseline_grid(ecl):
+def cpu_baseline_grid(g):
     orc = _orc()
-    g = grid_graph(ecl)
     e, t, cores = 0, 0.0, 1
     while t < 2.0:
         de, dt, cores = cpu_grid_once(g, orc)
@@ -819,9 +897,10 @@ def cpu_apsp_once(g, orc, ref):
     return float(g.nodes) ** 3, time.perf_counter() - t0, "port"
 
 
-def cpu_baseline_apsp(ecl):
-    g = apsp_graph(ecl, APSP_CPU_N)
-    u, t, kind = cpu_apsp_once(g, _orc(), _ref())
+def cpu_baseline_apsp():
+    orc = _orc()
+    g = apsp_graph(orc, APSP_CPU_N)
+    u, t, kind = cpu_apsp_once(g, orc, _ref())
     return {"value": u / t, "unit": "updates/s", "cores": 1, "kind": kind,
             "sample": f"one serial closure on an ER graph with n={APSP_CPU_N} (same expected degree and weights), "
                       f"{'reference FW_cpu' if kind == 'reference' else 'C oracle'}, {t:.1f} s"}
@@ -857,7 +936,7 @@ def reference_gpu_apsp(g):
             "note": "reference FW_gpu_64 (nvcc -O3 sm_100a), same graph, its printed compute time"}
 
 
-def reference_gpu(ecl, sym, dirg):
+def reference_gpu(sym, dirg):
     """The reference's race-free CUDA build (oracle/_ref) on the same graphs:
     kernel time as each reference driver times it."""
     import numpy as np
@@ -885,6 +964,8 @@ def reference_gpu(ecl, sym, dirg):
     di, dl = torch.from_numpy(dirg.nindex).cuda(), torch.from_numpy(dirg.nlist).cuda()
     scr = torch.empty(ref.eclref_scc_scratch_bytes(dirg.nodes, dirg.edges) // 8 + 2, dtype=torch.int64, device="cuda")
     res["scc"] = min(ref.eclref_scc_device(dirg.nodes, dirg.edges, P(di), P(dl), None, P(scr)) for _ in range(2))
+    del di, dl, scr
+    torch.cuda.empty_cache()
     edges = {"cc": sym.edges, "mis": sym.edges, "gc": sym.edges, "mst": sym.edges, "scc": dirg.edges}
     tot_e = sum(edges.values())
     tot_ms = sum(res.values())
@@ -893,95 +974,128 @@ def reference_gpu(ecl, sym, dirg):
             "note": "reference race-free CUDA build (nvcc -O3 sm_100a), same graphs, its own timed regions"}
 
 
-def run_reference_small(args, ecl):
+def _reference_line(args, metric, value, unit, ms_per_step, wl, cpu, gpu, world):
+    return {
+        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators: R-MAT / grid / Erdos-Renyi)",
+        "config": {"workload": wl, "l2": L2_NOTE}, "parallelism": "host cores (rank 0 only)",
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu": gpu,
+    }
+
+
+SUITE_METRIC = "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)"
+APSP_METRIC = "updates/s (n^3 / compute time of the blocked Floyd-Warshall closure; inputs resident)"
+
+
+def reference_small(args, workload, world):
     """Reference arm of the grid and APSP workloads."""
     orc, ref = _orc(), _ref()
-    if args.workload == "grid":
-        g = grid_graph(ecl)
-        for _ in range(min(args.warmup, 1)):
+    if workload == "grid":
+        g = grid_graph(orc)
+        for _ in range(args.warmup):
             cpu_grid_once(g, orc)
         u, t, gcores = 0.0, 0.0, 1
         for _ in range(args.steps):
             du, dt, gcores = cpu_grid_once(g, orc)
             u, t = u + du, t + dt
-        kind, unit = "port", "edges/s"
-        sample = f"the full 1024x1024 grid, the faster of the serial oracle CC and its OpenMP rendering ({gcores} thread(s))"
-        wl = f"grid1024-cc (n={g.nodes}, m={g.edges})"
-        metric = "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)"
+        kind, unit, cores = "port", "edges/s", gcores
+        sample = (f"the full 1024x1024 grid, the faster of the serial oracle CC and its OpenMP rendering "
+                  f"({gcores} thread(s)); the reference has no CPU CC solver")
+        wl, metric = grid_name(g), SUITE_METRIC
         try:
             gpu = reference_gpu_grid(g)
         except Exception as ex:
             gpu = {"error": str(ex)}
     else:
-        g = apsp_graph(ecl, APSP_CPU_N)
+        full = apsp_graph(orc)
+        g = apsp_graph(orc, APSP_CPU_N)
         u, t, kind = 0.0, 0.0, "port"
         for _ in range(args.steps):  # no warm-up: each closure takes seconds
             du, dt, kind = cpu_apsp_once(g, orc, ref)
             u, t = u + du, t + dt
-        unit = "updates/s"
-        sample = f"serial closure on ER n={APSP_CPU_N} ({'reference FW_cpu' if kind == 'reference' else 'C oracle'})"
-        wl = "er8192-apsp (CPU sample: n=%d)" % APSP_CPU_N
-        metric = "updates/s (n^3 / compute time of the blocked Floyd-Warshall closure; inputs resident)"
+        unit, cores = "updates/s", 1
+        sample = (f"serial closure on ER n={APSP_CPU_N}, same expected degree and weights "
+                  f"({'reference FW_cpu' if kind == 'reference' else 'C oracle'}); one closure per step")
+        wl, metric = apsp_name(full), APSP_METRIC
         try:
-            gpu = reference_gpu_apsp(apsp_graph(ecl))
+            gpu = reference_gpu_apsp(full)
         except Exception as ex:
             gpu = {"error": str(ex)}
     value = u / t
-    line = {
-        "impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generators)",
-        "config": {"workload": wl, "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": unit, "cores": gcores if args.workload == "grid" else 1,
-                         "kind": kind, "sample": sample},
-        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_gpu": gpu,
-    }
-    print(json.dumps(line), flush=True)
+    cpu = {"value": value, "unit": unit, "cores": cores, "kind": kind, "sample": sample}
+    return _reference_line(args, metric, value, unit, 1e3 * t / args.steps, wl, cpu, gpu, world)
+
+
+def reference_suite(args, world):
+    """Reference arm of the R-MAT suite, on the same R-MAT-22 graphs as our
+    arm.  A step is a bounded sample of the suite: ONE code, round robin over
+    CC, MIS, GC, MST, SCC, so that K steps cover every code about K/5 times
+    (with fewer than 5 steps every step runs the whole suite).  value = one
+    pass's edges over the sum of each code's mean time, the suite metric."""
+    orc, ref = _orc(), _ref()
+    sym, dirg = make_suite_graphs(orc, args.scale)
+    whole = args.steps < len(SUITE_LEGS)
+
+    def step(i, times, kinds, cores, edges):
+        t = 0.0
+        for code in (SUITE_LEGS if whole else (SUITE_LEGS[i % len(SUITE_LEGS)],)):
+            edges[code], dt, kinds[code], cores[code] = suite_leg(orc, ref, code, sym, dirg)
+            times.setdefault(code, []).append(dt)
+            t += dt
+        return t
+
+    for i in range(args.warmup):
+        step(i, {}, {}, {}, {})
+    times, kinds, cores, edges = {}, {}, {}, {}
+    t_tot = sum(step(i, times, kinds, cores, edges) for i in range(args.steps))
+    value = suite_rate(times, edges)
+    cpu = {"value": value, "unit": "edges/s", "cores": max(cores.values()), "kind": overall_kind(kinds),
+           "sample": "the suite on the same R-MAT-22 graphs, one code per step round robin: MST by the reference's "
+                     "own serial cpuMST; CC/MIS/GC/SCC (no CPU solver in the reference) by the faster of the serial "
+                     f"C oracle and its OpenMP rendering ({orc.omp_threads()} threads) on this host",
+           "per_code_kind": kinds, "per_code_cores": cores,
+           "per_code_mean_s": {c: round(sum(v) / len(v), 3) for c, v in times.items()}}
+    try:
+        gpu = reference_gpu(sym, dirg)
+    except Exception as ex:  # reported, not fatal: the CPU arm is the reference arm
+        gpu = {"error": str(ex)}
+    return _reference_line(args, SUITE_METRIC, value, "edges/s", 1e3 * t_tot / args.steps,
+                           suite_name(args.scale, sym, dirg), cpu, gpu, world)
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    import ecl_b200 as ecl
-
-    if args.workload in ("grid", "apsp"):
-        return run_reference_small(args, ecl)
-
-    orc = _orc()
-    ref = _ref()
-    scale = min(args.scale, 20)  # a bounded sample of the workload for the serial CPU codes
-    sym, dirg = make_suite_graphs(ecl, scale)
-    for _ in range(min(args.warmup, 1)):
-        cpu_suite_once(ecl, sym, dirg, orc, ref)
-    e_tot, t_tot, kinds, cores = 0, 0.0, {}, {}
-    for _ in range(args.steps):
-        e, t, kinds, cores = cpu_suite_once(ecl, sym, dirg, orc, ref)
-        e_tot += e
-        t_tot += t
-    value = e_tot / t_tot
-    gpu = None
-    try:
-        big_sym, big_dir = make_suite_graphs(ecl, args.scale)
-        gpu = reference_gpu(ecl, big_sym, big_dir)
-    except Exception as ex:  # reported, not fatal: the CPU arm is the reference arm
-        gpu = {"error": str(ex)}
-    line = {
-        "impl": "reference",
-        "metric": "edges/s (sum of g.edges over the suite's solves / sum of solve times; kernel time, inputs resident)",
-        "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t_tot / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "int32", "data": "synthetic (seeded generators)",
-        "config": {"workload": f"rmat{args.scale}-suite (CPU sample: R-MAT-{scale})", "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": max(cores.values()),
-                         "kind": "reference" if kinds.get("mst") == "reference" else "port",
-                         "sample": f"CPU suite on R-MAT-{scale}: MST = reference cpuMST (serial); CC/MIS/GC/SCC = the "
-                                   f"faster of the serial C oracle and its OpenMP rendering on this host",
-                         "per_code_kind": kinds, "per_code_cores": cores},
-        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_gpu": gpu,
-    }
+    if args.workload in ("batch", "serve"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched or served mode: each "
+                          "ECL code is a standalone executable that solves one graph per process"}), flush=True)
+        return
+    if args.workload == "suite":
+        line = reference_suite(args, world)
+        if world == 1 and args.other_configs:
+            sub = argparse.Namespace(**vars(args))
+            sub.steps, sub.warmup = min(args.steps, 5), min(args.warmup, 1)
+            line["other_configs"] = {w: reference_small(sub, w, world) for w in ("grid", "apsp")}
+    else:
+        line = reference_small(args, args.workload, world)
     print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    if args.workload == "batch":
+        line = bench_batch(args, rank, world, local_rank)
+    elif args.workload == "serve":
+        line = bench_serve(args, rank, world, local_rank)
+    else:
+        line = bench_plain(args, rank, world, local_rank)
+        # the other configs on one GPU only: a scaling run times the suite
+        if args.workload == "suite" and world == 1 and args.other_configs:
+            line["other_configs"] = other_configs(args, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():

@@ -111,8 +111,7 @@ void drop_graph_exec(ecl_batch* b) {
 // Enqueues one full run (every code, every super-batch) on b->stream.
 ecl_status enqueue_run(ecl_batch* b) {
   DeviceInfo dev = b->dev;
-  dev.blocks_per_sm = b->tune.blocks_per_sm;
-  dev.mst_light_factor = b->tune.mst_light_factor;
+  apply_tune(&dev, b->tune);
   for (Super& s : b->sup) {
     ECL_CUDA_TRY(cudaMemsetAsync(s.status, 0, kStatusBytes * kCodes, b->stream));
     GraphDev g;
@@ -389,7 +388,7 @@ ecl_status ecl_batch_run(ecl_batch* b, ecl_opts* opts) {
 }
 
 ecl_status ecl_batch_set_tune(ecl_batch* b, const ecl_tune* t) {
-  if (!b || !t) return ECL_ERR_INVALID_ARG;
+  if (!b || !t || !ecl::tune_valid(*t)) return ECL_ERR_INVALID_ARG;
   b->tune = *t;
   ecl::drop_graph_exec(b);
   b->capture_failed = false;

@@ -33,6 +33,8 @@
 //    re-check the rest of the list without blocking -- so a hop along the
 //    chain costs one poll and a short re-check, not a rescan of the row
 //    (short rows: the same with a bit mask per lane).
+#include <algorithm>
+
 #include "csr_bins.cuh"
 #include "radix_sort.cuh"
 #include "solvers.cuh"
@@ -409,9 +411,185 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
   return __ffsll((long long)~used) - 1;
 }
 
+// ---- the hub core: the first ranks of the order, coloured in shared memory ----
+//
+// On R-MAT the longest priority chain (about 2700 vertices at scale 22)
+// runs almost entirely through the long rows at the front of the order:
+// about 2200 of its hops lie in the first 16k ranks and 2470 in the first 32k.
+// A hop through L2 costs a store, a poll and a wake-up (about 1.7 us); in one
+// CTA's shared memory it costs a few hundred cycles.  So the first `core`
+// ranks (core = min(long rows, cap)) are coloured by ONE CTA of 32 warps with
+// their colours in shared memory, indexed by rank: every higher-priority
+// entry of a core row is itself a core vertex (it has a smaller rank), so a
+// core row never waits on global memory.  Two small launches first rewrite
+// the core rows' entries in nl2 from vertex ids to ranks (rank[] is the
+// inverse of the order over the core), so the core reads its entries with
+// coalesced loads and looks their colours up in shared memory.  gc_pull then
+// starts its long rows after the core.
+constexpr int kCoreThreads = 1024;
+constexpr int kCoreWarps = kCoreThreads / 32;
+constexpr int kCorePend = 512;          // per-warp list of undecided entries
+constexpr int kCoreBatch = 4;           // entries per lane whose loads are in flight together
+constexpr int kCoreDefault = 32768;     // default core size (ranks)
+constexpr int kCoreMax = 36864;         // shared memory bound: colours + per-warp bitmaps and lists
+
+__host__ __device__ constexpr size_t gc_core_smem(int cap) {
+  return sizeof(int) * ((size_t)cap + (size_t)kCoreWarps * (kMexWords + kCorePend));
+}
+
+// Core size of this solve: the long rows (a prefix of the order), at most cap.
+__device__ __forceinline__ int gc_core_size(const GCCtl* ctl, int cap) { return min(ld(&ctl->nbig), cap); }
+
+// rank[order[r]] = r over the core.
+__global__ void __launch_bounds__(kTPB) gc_core_rank(const int* __restrict__ order, int* __restrict__ rank,
+                                                     const GCCtl* __restrict__ ctl, int cap) {
+  const int core = gc_core_size(ctl, cap);
+  for (int r = blockIdx.x * kTPB + threadIdx.x; r < core; r += gridDim.x * kTPB) rank[__ldg(&order[r])] = r;
+}
+
+// Rewrites the higher-priority entries of every core row from vertex ids to
+// ranks, one warp per row.  Such an entry outranks its row, so its rank is
+// below the row's and inside the core.
+__global__ void __launch_bounds__(kTPB) gc_core_translate(const int* __restrict__ nindex, int* __restrict__ nl2,
+                                                          const int* __restrict__ hc, const int* __restrict__ order,
+                                                          const int* __restrict__ rank, const GCCtl* __restrict__ ctl,
+                                                          int cap) {
+  const int lane = threadIdx.x & 31;
+  const int core = gc_core_size(ctl, cap);
+  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * kTPB) >> 5;
+  for (int r = warp; r < core; r += nwarps) {
+    const int v = __ldg(&order[r]);
+    const int b = __ldg(&nindex[v]), e = b + __ldg(&hc[v]);
+    for (int i = b + lane; i < e; i += 32) nl2[i] = __ldg(&rank[nl2[i]]);
+  }
+}
+
+// Colour in shared memory of core rank q once it is published; -1 when the
+// wait gives up (2 s without the colour, or another error raised).
+__device__ __forceinline__ int gc_core_wait(const int* col_s, int q, Status* status) {
+  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
+  int c = bref(*const_cast<int*>(&col_s[q])).load(cuda::memory_order_relaxed);
+  if (c >= 0) return c;
+  const unsigned long long t0 = gc_now();
+  for (unsigned spins = 1;; spins++) {
+    c = bref(*const_cast<int*>(&col_s[q])).load(cuda::memory_order_relaxed);
+    if (c >= 0) return c;
+    if ((spins & 1023u) == 0 && (gc_now() - t0 > kStallNs || ld(&status->code) != 0)) {
+      raise(status, ECL_ERR_NO_CONVERGENCE, q);
+      return -1;
+    }
+    // a short nap after the first polls leaves issue slots to the warps
+    // that are still scanning their rows
+    if (spins > 8) __nanosleep(32);
+  }
+}
+
+// Colour of core rank r whose entries (ranks) are nl2[wb, we): the smallest
+// colour none of them uses, by windows of 2048 colours.  One non-blocking
+// pass files the entries not coloured yet in `pend`; then each lane waits on
+// one listed entry at a time.  An entry outside [0, r) is not a
+// higher-priority core vertex: ECL_ERR_BAD_GRAPH.  Returns -1 on a stall.
+// All lanes call.
+__device__ int gc_core_row(int r, int wb, int we, const int* nl2, const int* col_s, unsigned* bits, int* pend,
+                           Status* status) {
+  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1;
+  for (int off = 0;; off += 32 * kMexWords) {
+    bits[lane] = 0;
+    bits[lane + 32] = 0;
+    __syncwarp();
+    int cursor = wb;
+    while (cursor < we) {
+      int np = 0;
+      int i0 = cursor;
+      for (; i0 < we && np + 32 * kCoreBatch <= kCorePend; i0 += 32 * kCoreBatch) {
+        int q[kCoreBatch], c[kCoreBatch];
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++) {
+          const int i = i0 + 32 * k + lane;
+          q[k] = i < we ? __ldg(&nl2[i]) : -1;
+          if (i < we && (unsigned)q[k] >= (unsigned)r) {
+            raise(status, ECL_ERR_BAD_GRAPH, r);
+            q[k] = -1;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++)
+          c[k] = q[k] >= 0 ? bref(*const_cast<int*>(&col_s[q[k]])).load(cuda::memory_order_relaxed) : 0;
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++) {
+          const bool undecided = q[k] >= 0 && c[k] < 0;
+          if (q[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
+          const unsigned ub = __ballot_sync(kFull, undecided);
+          if (undecided) pend[np + __popc(ub & lt)] = q[k];
+          np += __popc(ub);
+        }
+      }
+      cursor = i0;
+      __syncwarp();
+      bool stalled = false;
+      for (int j = lane; j < np; j += 32) {
+        const int c = gc_core_wait(col_s, pend[j], status);
+        if (c < 0) {
+          stalled = true;
+          break;
+        }
+        gc_mark(bits, c, off);
+      }
+      if (__any_sync(kFull, stalled)) return -1;
+    }
+    __syncwarp();
+    const unsigned w0 = bits[lane], w1 = bits[lane + 32];
+    const unsigned f0 = __ballot_sync(kFull, w0 != ~0u), f1 = __ballot_sync(kFull, w1 != ~0u);
+    int c = -1;
+    if (f0) {
+      const int wi = __ffs(f0) - 1;
+      c = off + wi * 32 + __ffs(~__shfl_sync(kFull, w0, wi)) - 1;
+    } else if (f1) {
+      const int wi = __ffs(f1) - 1;
+      c = off + (wi + 32) * 32 + __ffs(~__shfl_sync(kFull, w1, wi)) - 1;
+    }
+    __syncwarp();
+    if (c >= 0) return c;
+  }
+}
+
+// One CTA colours the core: rank r goes to warp r mod 32, each warp takes its
+// ranks in increasing order (the warp holding the lowest uncoloured rank can
+// always finish it), and every colour is published to shared memory for the
+// core and to color[] for gc_pull.
+__global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict__ nindex, const int* __restrict__ nl2,
+                                                           const int* __restrict__ hc, const int* __restrict__ order,
+                                                           int* __restrict__ color, const GCCtl* __restrict__ ctl,
+                                                           int cap, Status* __restrict__ status) {
+  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
+  extern __shared__ int s_core[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int core = gc_core_size(ctl, cap);
+  int* col_s = s_core;
+  unsigned* bits = reinterpret_cast<unsigned*>(s_core + cap) + warp * kMexWords;
+  int* pend = s_core + cap + kCoreWarps * kMexWords + warp * kCorePend;
+  for (int r = threadIdx.x; r < core; r += kCoreThreads) bref(col_s[r]).store(-1, cuda::memory_order_relaxed);
+  __syncthreads();
+  for (int r = warp; r < core; r += kCoreWarps) {
+    const int v = __ldg(&order[r]);
+    const int wb = __ldg(&nindex[v]);
+    const int c = gc_core_row(r, wb, wb + __ldg(&hc[v]), nl2, col_s, bits, pend, status);
+    if (c < 0) return;
+    if (lane == 0) {
+      bref(col_s[r]).store(c, cuda::memory_order_relaxed);
+      st(&color[v], c);
+    }
+    __syncwarp();
+  }
+}
+
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
                                                 const int* __restrict__ hc, const int* __restrict__ order,
-                                                int* __restrict__ color, GCCtl* __restrict__ ctl,
+                                                int* __restrict__ color, GCCtl* __restrict__ ctl, int core_cap,
                                                 Status* __restrict__ status) {
   __shared__ unsigned s_bits[kTPB / 32][kMexWords];
   __shared__ int s_pend[kTPB / 32][kPend];
@@ -429,7 +607,8 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   // Long rows, ONE per warp at a time: every long row in flight scans its
   // higher-priority list concurrently, so the dense hub core's rows all wait
   // at the same time instead of one after another.
-  for (int r = gwarp; r < nbig; r += nwarps) {
+  // ranks below the core size were coloured by gc_core
+  for (int r = gc_core_size(ctl, core_cap) + gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
     const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, status);
@@ -517,8 +696,17 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);
   const int* order = in1 ? b.vals1 : b.vals0;
   mark();
+  // the hub core (the sort keys are dead now: their buffer holds the ranks)
+  const int cap = std::min(std::min(dev.gc_core_ranks > 0 ? dev.gc_core_ranks : kCoreDefault, kCoreMax), g.n);
+  int* rank = reinterpret_cast<int*>(b.keys0);
+  ECL_LAUNCH(gc_core_rank, grid, kTPB, 0, stream, order, rank, b.ctl, cap);
+  ECL_LAUNCH(gc_core_translate, grid, kTPB, 0, stream, g.nindex, b.nl2, b.hc, order, rank, b.ctl, cap);
+  ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
+  ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, g.nindex, b.nl2, b.hc, order, color, b.ctl, cap,
+             status);
+  mark();
   ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
-                                  status));
+                                  cap, status));
   mark();
   return ECL_OK;
 }

@@ -14,7 +14,19 @@ namespace {
 thread_local std::string t_last_error;
 std::mutex g_dev_mu;
 DeviceInfo g_dev_cache[64];
+ecl_tune g_tune{};  // process-wide knobs of the single-graph entry points (under g_dev_mu)
 }  // namespace
+
+bool tune_valid(const ecl_tune& t) {
+  return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 8 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
+         t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864;
+}
+
+void apply_tune(DeviceInfo* d, const ecl_tune& t) {
+  d->blocks_per_sm = t.blocks_per_sm;
+  d->mst_light_factor = t.mst_light_factor;
+  d->gc_core_ranks = t.gc_core_ranks;
+}
 
 void set_last_error(const char* where, cudaError_t e) {
   char buf[512];
@@ -60,6 +72,7 @@ ecl_status current_device(DeviceInfo* info) {
     return ECL_ERR_NO_DEVICE;
   }
   *info = c;
+  apply_tune(info, g_tune);
   return ECL_OK;
 }
 
@@ -226,6 +239,20 @@ ecl_status Solve::finish(ecl_status st) {
 extern "C" {
 
 int32_t ecl_abi_version(void) { return ECL_B200_ABI_VERSION; }
+
+ecl_status ecl_set_tune(const ecl_tune* t) {
+  if (!t || !ecl::tune_valid(*t)) return ECL_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ecl::g_dev_mu);
+  ecl::g_tune = *t;
+  return ECL_OK;
+}
+
+ecl_status ecl_get_tune(ecl_tune* t) {
+  if (!t) return ECL_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(ecl::g_dev_mu);
+  *t = ecl::g_tune;
+  return ECL_OK;
+}
 
 const char* ecl_status_string(ecl_status s) {
   switch (s) {

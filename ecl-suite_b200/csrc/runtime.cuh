@@ -68,12 +68,17 @@ struct DeviceInfo {
   // Tunable launch knobs (0 = default), set by the batched engine's autotuner.
   int blocks_per_sm = 0;
   float mst_light_factor = 0.f;
+  int gc_core_ranks = 0;  // GC: ranks coloured in one CTA's shared memory (0 = default)
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }
 };
-// Properties of the current device (cached per device id).
+// Properties of the current device (cached per device id), with the
+// process-wide knobs of ecl_set_tune applied.
 ecl_status current_device(DeviceInfo* info);
+// Range check of a knob set, and its application to a DeviceInfo.
+bool tune_valid(const ecl_tune& t);
+void apply_tune(DeviceInfo* d, const ecl_tune& t);
 
 // Workspace carving: the same sequence of take() calls sizes a workspace
 // (base == nullptr) and then hands out 256-byte-aligned sub-buffers.

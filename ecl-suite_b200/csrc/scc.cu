@@ -10,14 +10,14 @@
 // is the largest vertex id of v's SCC -- schedule independent.
 //
 // B200 design:
-//  * scc_mark / scc_build trim first: a vertex with no in-entry or no
-//    out-entry (self-loops ignored) is its own SCC and contributes no edge.
-//    scc_build writes the int2 edge list in CSR positions -- slot i holds
-//    (v, nlist[i]) when both ends are live, else a dead slot -- so it is one
-//    streaming pass with no shared append counter (on R-MAT nearly every
-//    edge survives the trim, so compacting it would buy nothing).  Both
-//    passes are degree-binned (lane / warp / 256-entry chunk records), so
-//    hub rows spread over all warps;
+//  * scc_mark trims first: a vertex with no in-entry or no out-entry
+//    (self-loops ignored) is its own SCC and contributes no edge.  The same
+//    pass writes the int2 edge list in CSR positions -- slot i holds
+//    (v, nlist[i]), or a dead slot for a self-loop or a bad id -- so the list
+//    costs one streaming store per entry and no separate pass (on R-MAT nearly
+//    every edge survives the trim, so compacting it would buy nothing).  Rows
+//    are degree-binned (lane / warp / 256-entry chunk records), so hub rows
+//    spread over all warps;
 //  * scc_solve runs EVERY propagation sweep and every trimming round in one
 //    cooperative persistent launch, separated by bounded grid barriers (the
 //    reference pays a host round trip per propagation launch, :283-287).
@@ -25,7 +25,8 @@
 //    max low), like the reference's iomax, so an edge costs two word loads
 //    plus two for the jumps io[in-max(v)] / io[out-max(w)] (both still valid
 //    bounds, so values travel many hops per sweep); a raise is a 32-bit
-//    atomic max on one half;
+//    atomic max on one half.  Trimmed vertices hold a DEAD word that every
+//    sweep skips.  Each lane keeps kSweepBatch edges' loads in flight;
 //  * rounds after the first compact the surviving edges (the edges whose two
 //    ends share both values and are unresolved: io[v] == io[w]);
 //  * the final labels are written by the same launch (label = in-max).
@@ -79,13 +80,16 @@ __device__ __forceinline__ bool io_raise(unsigned long long* p, unsigned long lo
 // with such an entry; rows longer than kBinChunk go to chunk records.
 constexpr int kHasIn = 1, kHasOut = 2;
 
-// Marks kScanBatch entries w[k] (present where valid[k]) of v's list: v has
-// an out-entry and each w an in-entry (self-loops ignored).  The flag words
-// are read first and OR'ed only where kHasIn is still clear: R-MAT sends a
-// large share of all entries to a few hub ids, whose words would otherwise
-// take an atomic from every one of them.
+// Marks kScanBatch entries w[k] (present where valid[k]) of v's list, at CSR
+// positions j[k]: v has an out-entry and each w an in-entry (self-loops
+// ignored), and slot j[k] of the edge list becomes (v, w) -- or a dead slot
+// for a self-loop or an id out of range.  The flag words are read first and
+// OR'ed only where kHasIn is still clear: R-MAT sends a large share of all
+// entries to a few hub ids, whose words would otherwise take an atomic from
+// every one of them.
 __device__ __forceinline__ void scc_mark_batch(const bool (&valid)[kScanBatch], int v, const int (&w)[kScanBatch],
-                                               int n, int* flags, bool& out, Status* status) {
+                                               const int (&j)[kScanBatch], int n, int* flags, int2* wl, bool& out,
+                                               Status* status) {
   int f[kScanBatch];
 #pragma unroll
   for (int k = 0; k < kScanBatch; k++)
@@ -93,43 +97,41 @@ __device__ __forceinline__ void scc_mark_batch(const bool (&valid)[kScanBatch], 
 #pragma unroll
   for (int k = 0; k < kScanBatch; k++) {
     if (!valid[k]) continue;
-    if ((unsigned)w[k] >= (unsigned)n) {
-      raise(status, ECL_ERR_BAD_GRAPH, w[k]);
-    } else if (w[k] != v) {
+    const bool edge = (unsigned)w[k] < (unsigned)n && w[k] != v;
+    if ((unsigned)w[k] >= (unsigned)n) raise(status, ECL_ERR_BAD_GRAPH, w[k]);
+    if (edge) {
       if (!(f[k] & kHasIn)) fetch_or(&flags[w[k]], kHasIn);
       out = true;
     }
+    __stcs(&wl[j[k]], edge ? make_int2(v, w[k]) : make_int2(-1, -1));
   }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __restrict__ nindex,
                                                  const int* __restrict__ nlist, int* __restrict__ flags,
-                                                 unsigned long long* __restrict__ io,
-                                                 RowChunks rc, Status* __restrict__ status) {
+                                                 int2* __restrict__ wl, RowChunks rc, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   for (int base = warp * 32; base < n; base += nwarps * 32) {
     const int v = base + lane;
     int beg = 0, end = 0;
-    if (v < n) {
-      csr_row(nindex, v, m, beg, end, status);
-      io[v] = io_pack(v, v);
-    }
+    if (v < n) csr_row(nindex, v, m, beg, end, status);
     const int deg = end - beg;
     push_chunks_warp<kBinChunk>(rc, deg > kBinChunk, v, beg, end, status);
     bool out = false;
     const bool lanelvl = deg <= kBinLane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch) {
-      int w[kScanBatch];
+      int w[kScanBatch], j[kScanBatch];
       bool valid[kScanBatch];
 #pragma unroll
       for (int k = 0; k < kScanBatch; k++) {
         valid[k] = lanelvl && k0 + k < deg;
-        w[k] = valid[k] ? __ldg(&nlist[beg + k0 + k]) : 0;
+        j[k] = beg + k0 + k;
+        w[k] = valid[k] ? __ldg(&nlist[j[k]]) : 0;
       }
-      scc_mark_batch(valid, v, w, n, flags, out, status);
+      scc_mark_batch(valid, v, w, j, n, flags, wl, out, status);
     }
     unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
     while (todo) {
@@ -140,14 +142,15 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       const int wend = __shfl_sync(kFull, end, who);
       bool wout = false;
       for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) {
-        int w[kScanBatch];
+        int w[kScanBatch], j[kScanBatch];
         bool valid[kScanBatch];
 #pragma unroll
         for (int k = 0; k < kScanBatch; k++) {
-          valid[k] = i0 + 32 * k < wend;
-          w[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k]) : 0;
+          j[k] = i0 + 32 * k;
+          valid[k] = j[k] < wend;
+          w[k] = valid[k] ? __ldg(&nlist[j[k]]) : 0;
         }
-        scc_mark_batch(valid, wv, w, n, flags, wout, status);
+        scc_mark_batch(valid, wv, w, j, n, flags, wl, wout, status);
       }
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
 
 __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
                                                         const int* __restrict__ nlist, int* __restrict__ flags,
-                                                        RowChunks rc,
+                                                        int2* __restrict__ wl, RowChunks rc,
                                                         Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -168,103 +171,39 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
     for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) {
-      int w[kScanBatch];
+      int w[kScanBatch], j[kScanBatch];
       bool valid[kScanBatch];
 #pragma unroll
       for (int k = 0; k < kScanBatch; k++) {
-        valid[k] = i0 + 32 * k < end;
-        w[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k]) : 0;
+        j[k] = i0 + 32 * k;
+        valid[k] = j[k] < end;
+        w[k] = valid[k] ? __ldg(&nlist[j[k]]) : 0;
       }
-      scc_mark_batch(valid, r.x, w, n, flags, out, status);
+      scc_mark_batch(valid, r.x, w, j, n, flags, wl, out, status);
     }
     if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
   }
 }
 
-__device__ __forceinline__ bool scc_live(const int* flags, int v) {
-  return ld(&flags[v]) == (kHasIn | kHasOut);
-}
-
-// Writes the edge-list slots of kScanBatch CSR entries of v per lane: entry
-// k is j0 + k * stride when below jend.  The list entries, then the flag words
-// of their targets, are loaded before any slot is written.
-__device__ __forceinline__ void scc_slots(int j0, int stride, int jend, bool live_v, int v, int n,
-                                          const int* nlist, const int* flags, int2* wl) {
-  int w[kScanBatch], f[kScanBatch];
-#pragma unroll
-  for (int k = 0; k < kScanBatch; k++) {
-    const int j = j0 + k * stride;
-    w[k] = j < jend ? __ldg(&nlist[j]) : -1;
-  }
-#pragma unroll
-  for (int k = 0; k < kScanBatch; k++)
-    f[k] = (live_v && (unsigned)w[k] < (unsigned)n && w[k] != v) ? ld(&flags[w[k]]) : 0;
-#pragma unroll
-  for (int k = 0; k < kScanBatch; k++) {
-    const int j = j0 + k * stride;
-    if (j < jend) wl[j] = f[k] == (kHasIn | kHasOut) ? make_int2(v, w[k]) : make_int2(-1, -1);
-  }
-}
-
-__global__ void __launch_bounds__(kTPB) scc_build(int n, int m, const int* __restrict__ nindex,
-                                                  const int* __restrict__ nlist, const int* __restrict__ flags,
-                                                  int2* __restrict__ wl) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * kTPB) >> 5;
-  for (int base = warp * 32; base < n; base += nwarps * 32) {
-    const int v = base + lane;
-    int beg = 0, end = 0;
-    bool live = false;
-    if (v < n) {
-      beg = __ldg(&nindex[v]);
-      end = __ldg(&nindex[v + 1]);
-      if (beg < 0 || end < beg || end > m) beg = end = 0;  // reported by scc_mark
-      live = scc_live(flags, v);
-    }
-    const int deg = end - beg;
-    const bool lanelvl = deg <= kBinLane;
-    const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
-    for (int k0 = 0; k0 < kmax; k0 += kScanBatch)
-      if (lanelvl) scc_slots(beg + k0, 1, end, live, v, n, nlist, flags, wl);
-    unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
-    while (todo) {
-      const int who = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int wv = __shfl_sync(kFull, v, who);
-      const int wbeg = __shfl_sync(kFull, beg, who);
-      const int wend = __shfl_sync(kFull, end, who);
-      const bool wlive = __shfl_sync(kFull, live, who);
-      for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) scc_slots(i0, 32, wend, wlive, wv, n, nlist, flags, wl);
-    }
-  }
-}
-
-__global__ void __launch_bounds__(kTPB) scc_build_chunks(int n, const int* __restrict__ nindex,
-                                                         const int* __restrict__ nlist, const int* __restrict__ flags,
-                                                         int2* __restrict__ wl,
-                                                         RowChunks rc) {
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * kTPB) >> 5;
-  const int total = chunk_total(rc);
-  for (int c = warp; c < total; c += nwarps) {
-    const int2 r = rc.rec[c];
-    const bool live = scc_live(flags, r.x);
-    const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
-    for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) scc_slots(i0, 32, end, live, r.x, n, nlist, flags, wl);
-  }
-}
+// Word of a trimmed vertex: it is its own SCC, and sweeps skip its edges.
+constexpr unsigned long long kDead = ~0ull;
+// Edges per lane whose loads are issued together in a sweep.
+constexpr int kSweepBatch = 4;
 
 // Round 0 sweeps the CSR-position edge list of `m0` slots (dead slots have
 // x < 0); later rounds sweep the compacted survivors.
-__global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
-                                                  unsigned long long* __restrict__ io, int* __restrict__ label,
-                                                  SCCCtl* __restrict__ ctl, SCCRound* __restrict__ rounds,
-                                                  int max_rounds, Status* __restrict__ status) {
+__global__ void __launch_bounds__(kTPB, 4) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
+                                                  const int* __restrict__ flags, unsigned long long* __restrict__ io,
+                                                  int* __restrict__ label, SCCCtl* __restrict__ ctl,
+                                                  SCCRound* __restrict__ rounds, int max_rounds,
+                                                  Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int tid = blockIdx.x * kTPB + threadIdx.x;
   const int nthreads = gridDim.x * kTPB;
+  // 0. live vertices start at (v, v); trimmed ones are DEAD
+  for (int v = tid; v < n; v += nthreads)
+    io[v] = __ldg(&flags[v]) == (kHasIn | kHasOut) ? io_pack(v, v) : kDead;
+  if (!grid_sync(&ctl->bar, status)) return;
   int size = m0;
   int sweep = 0;
   int round = 0;
@@ -288,40 +227,59 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restric
       // same word as every other edge.  A value read earlier is a smaller
       // but still valid bound (in-max and out-max only grow).
       int c_iv = -1, c_in = -1, c_ow = -1, c_out = -1;
-      // Whole warps step together: in CSR order neighbouring lanes mostly
-      // share v, so the out-max raises of v are combined per warp
-      // (__match_any_sync + max) into one atomic instead of up to 32 on one
-      // address.
-      for (int i0 = tid - lane; i0 < size; i0 += nthreads) {
-        const int i = i0 + lane;
-        const int2 e = i < size ? cur[i] : make_int2(-1, -1);
-        const int v = e.x, w = e.y;
-        unsigned long long A = 0;
-        int ow = -1;
-        if (v >= 0) {
-          A = ld(&io[v]);
-          const unsigned long long B = ld(&io[w]);
-          int iv = io_in(A);
-          if (iv != v) {
-            if (iv != c_iv) {
-              c_iv = iv;
-              c_in = io_in(ld(&io[iv]));
-            }
-            iv = max(iv, c_in);
-          }
-          ow = io_out(B);
-          if (ow != w) {
-            if (ow != c_ow) {
-              c_ow = ow;
-              c_out = io_out(ld(&io[ow]));
-            }
-            ow = max(ow, c_out);
-          }
-          if (io_raise<true>(&io[w], B, iv)) moved = true;
+      // Whole warps step together over kSweepBatch slices of 32 consecutive
+      // slots; in CSR order neighbouring lanes mostly share v, so the out-max
+      // raises of v are combined per slice (__match_any_sync + max) into one
+      // atomic instead of up to 32 on one address.  Each lane's edge records,
+      // then their io words, then the jump words are loaded before any is
+      // used.
+      for (int i0 = (tid - lane) * kSweepBatch; i0 < size; i0 += nthreads * kSweepBatch) {
+        int2 e[kSweepBatch];
+#pragma unroll
+        for (int k = 0; k < kSweepBatch; k++) {
+          const int i = i0 + 32 * k + lane;
+          e[k] = i < size ? __ldcs(&cur[i]) : make_int2(-1, -1);
+          if ((unsigned)e[k].x >= (unsigned)n || (unsigned)e[k].y >= (unsigned)n) e[k] = make_int2(-1, -1);
         }
-        const unsigned grp = __match_any_sync(kFull, v);
-        const int gow = __reduce_max_sync(grp, ow);
-        if (v >= 0 && lane == __ffs(grp) - 1 && io_raise<false>(&io[v], A, gow)) moved = true;
+        unsigned long long A[kSweepBatch], B[kSweepBatch];
+#pragma unroll
+        for (int k = 0; k < kSweepBatch; k++) {
+          A[k] = e[k].x >= 0 ? ld(&io[e[k].x]) : kDead;
+          B[k] = e[k].x >= 0 ? ld(&io[e[k].y]) : kDead;
+        }
+        // jumps not covered by the memo load only the half they need (in-max
+        // is the high word); -1 = not loaded (live values are >= 0)
+        int iv[kSweepBatch], ow[kSweepBatch], ji[kSweepBatch], jo[kSweepBatch];
+#pragma unroll
+        for (int k = 0; k < kSweepBatch; k++) {
+          const bool live = A[k] != kDead && B[k] != kDead;
+          iv[k] = live ? io_in(A[k]) : -1;
+          ow[k] = live ? io_out(B[k]) : -1;
+          ji[k] = (live && iv[k] != e[k].x && iv[k] != c_iv) ? ld(reinterpret_cast<const int*>(&io[iv[k]]) + 1) : -1;
+          jo[k] = (live && ow[k] != e[k].y && ow[k] != c_ow) ? ld(reinterpret_cast<const int*>(&io[ow[k]])) : -1;
+        }
+#pragma unroll
+        for (int k = 0; k < kSweepBatch; k++) {
+          if (iv[k] >= 0 && iv[k] != e[k].x) {
+            if (ji[k] >= 0) {
+              c_iv = iv[k];
+              c_in = ji[k];
+            }
+            if (iv[k] == c_iv) iv[k] = max(iv[k], c_in);
+          }
+          if (ow[k] >= 0 && ow[k] != e[k].y) {
+            if (jo[k] >= 0) {
+              c_ow = ow[k];
+              c_out = jo[k];
+            }
+            if (ow[k] == c_ow) ow[k] = max(ow[k], c_out);
+          }
+          if (iv[k] >= 0 && io_raise<true>(&io[e[k].y], B[k], iv[k])) moved = true;
+          const int v = iv[k] >= 0 ? e[k].x : -1;
+          const unsigned grp = __match_any_sync(kFull, v);
+          const int gow = __reduce_max_sync(grp, ow[k]);
+          if (v >= 0 && lane == __ffs(grp) - 1 && io_raise<false>(&io[v], A[k], gow)) moved = true;
+        }
       }
       if (__any_sync(kFull, moved) && lane == 0) st(&ctl->changed[sweep], 1);
       if (!grid_sync(&ctl->bar, status)) return;
@@ -336,20 +294,22 @@ __global__ void __launch_bounds__(kTPB) scc_solve(int n, int m0, int2* __restric
       int2 e = make_int2(0, 0);
       if (i < size) {
         e = cur[i];
-        if (e.x >= 0) {
+        if ((unsigned)e.x < (unsigned)n && (unsigned)e.y < (unsigned)n) {
           const unsigned long long A = ld(&io[e.x]);
-          keep = io_in(A) != io_out(A) && A == ld(&io[e.y]);
+          keep = A != kDead && io_in(A) != io_out(A) && A == ld(&io[e.y]);
         }
       }
       const int at = warp_append(&rounds[round].size, keep);
       if (keep) nxt[at] = e;
     }
     if (!grid_sync(&ctl->bar, status)) return;
-    // 3. retire resolved vertices, reset the rest to their own id
+    // 3. retire resolved (and trimmed) vertices, reset the rest to their own id
     bool again = false;
     for (int v = tid; v < n; v += nthreads) {
       const unsigned long long A = ld(&io[v]);
-      if (io_in(A) == io_out(A)) {
+      if (A == kDead) {
+        label[v] = v;
+      } else if (io_in(A) == io_out(A)) {
         label[v] = io_in(A);
       } else {
         st(&io[v], io_pack(v, v));
@@ -422,14 +382,11 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaMemsetAsync(b.flags, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m)};
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.io, rc, status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, rc, status);
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, status);
   mark();
-  ECL_LAUNCH(scc_build, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA);
-  ECL_LAUNCH(scc_build_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc);
-  mark();
-  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.io, label, b.ctl,
-                                  b.rounds, max_rounds, status));
+  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label,
+                                  b.ctl, b.rounds, max_rounds, status));
   mark();
   return ECL_OK;
 }

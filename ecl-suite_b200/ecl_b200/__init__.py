@@ -118,7 +118,7 @@ _sig("ecl_gen_er", C.c_int, [_I32, _F64, _U64, _I32, _U64, _I32, _I32, _PG])
 # Every symbol that include/ecl_b200.h declares (checked by the CPU tests).
 EXPORTED = [
     "ecl_abi_version", "ecl_status_string", "ecl_last_error", "ecl_workspace_bytes", "ecl_kernel_launches",
-    "ecl_minplus_peak",
+    "ecl_minplus_peak", "ecl_set_tune", "ecl_get_tune",
     "ecl_cc", "ecl_mis", "ecl_gc", "ecl_mst", "ecl_scc", "ecl_apsp",
     "ecl_compute_cc", "ecl_compute_mis", "ecl_compute_gc", "ecl_compute_mst", "ecl_compute_scc", "ecl_compute_apsp",
     "ecl_graph_read", "ecl_graph_write", "ecl_graph_free", "ecl_graph_validate",
@@ -382,7 +382,34 @@ BATCH_CC, BATCH_MIS, BATCH_GC, BATCH_MST, BATCH_SCC = 0x1, 0x2, 0x4, 0x8, 0x10
 
 
 class Tune(C.Structure):
-    _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float)]
+    """ecl_tune: launch knobs (0 = built-in default); they never change results."""
+
+    _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float), ("gc_core_ranks", C.c_int32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_sig("ecl_set_tune", C.c_int, [C.POINTER(Tune)])
+_sig("ecl_get_tune", C.c_int, [C.POINTER(Tune)])
+
+
+def get_tune() -> Tune:
+    t = Tune()
+    _check(lib.ecl_get_tune(C.byref(t)), "ecl_get_tune")
+    return t
+
+
+def set_tune(t: Optional[Tune] = None, **knobs) -> Tune:
+    """Sets the process-wide knobs of the single-graph solvers (unnamed knobs
+    keep their current values); returns the previous setting."""
+    old = get_tune()
+    new = Tune()
+    C.memmove(C.byref(new), C.byref(t if t is not None else old), C.sizeof(Tune))
+    for k, v in knobs.items():
+        setattr(new, k, v)
+    _check(lib.ecl_set_tune(C.byref(new)), "ecl_set_tune")
+    return old
 
 
 _PB = C.c_void_p
@@ -412,10 +439,14 @@ class Batch:
         _check(lib.ecl_batch_create(C.byref(h)), "ecl_batch_create")
         self.h = h
 
-    def __del__(self):
+    def close(self):
+        """Releases the engine's device memory now (also done on garbage collection)."""
         if getattr(self, "h", None):
             lib.ecl_batch_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     def add(self, g: Graph):
         v = g.view()
@@ -432,10 +463,10 @@ class Batch:
         _check(lib.ecl_batch_run(self.h, C.byref(o)), "ecl_batch_run")
         return o.elapsed_ms, bool(o.rounds)
 
-    def tune(self, trials=2):
+    def tune(self, trials=2) -> Tune:
         t = Tune()
         _check(lib.ecl_batch_tune(self.h, trials, C.byref(t)), "ecl_batch_tune")
-        return t.blocks_per_sm, t.mst_light_factor
+        return t
 
     @property
     def graphs(self) -> int:
@@ -522,10 +553,14 @@ class Server:
         _check(lib.ecl_server_create(C.byref(cfg), C.byref(h)), "ecl_server_create")
         self.h = h
 
-    def __del__(self):
+    def close(self):
+        """Releases the resident graphs and the server's streams now (also on garbage collection)."""
         if getattr(self, "h", None):
             lib.ecl_server_destroy(self.h)
             self.h = None
+
+    def __del__(self):
+        self.close()
 
     def add_graph(self, g: Graph) -> int:
         gid = C.c_int32()

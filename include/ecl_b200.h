@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define ECL_B200_ABI_VERSION 1
+#define ECL_B200_ABI_VERSION 2
 
 typedef enum ecl_status {
   ECL_OK = 0,
@@ -79,6 +79,24 @@ typedef struct ecl_opts {
   int32_t nphases;        /* out: number of phase_ms entries written */
   float phase_ms[8];      /* out: device time of each kernel phase, in launch order */
 } ecl_opts;
+
+/* Launch knobs: how the solvers schedule their work, never what they compute
+ * (0 = built-in default).  The reference fixes the matching choices at compile
+ * time: CC's per-thread / per-warp / per-block row thresholds
+ * (ECL-CC-atomic.cu:62,120,122), GC's block size and warp rows
+ * (ECL-GC-atomic.cu:60-64,93), MST's warp path and light-edge sample
+ * (ECL-MST_10-atomic.cu:197,450-459). */
+typedef struct ecl_tune {
+  int32_t blocks_per_sm;  /* blocks of 256 threads per SM for the grid-stride kernels; 0 = fill the SM */
+  float mst_light_factor; /* MST light-edge target, in multiples of n; 0 = 0.75 */
+  int32_t gc_core_ranks;  /* GC: leading ranks coloured in one CTA's shared memory, 0..36864; 0 = 32768 */
+} ecl_tune;
+
+/* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);
+ * the batched engine keeps its own (ecl_batch_set_tune).  Out-of-range values
+ * give ECL_ERR_INVALID_ARG and change nothing. */
+ecl_status ecl_set_tune(const ecl_tune* t);
+ecl_status ecl_get_tune(ecl_tune* t);
 
 /* Solver identifiers (ecl_workspace_bytes). */
 typedef enum ecl_code { ECL_CC = 0, ECL_MIS = 1, ECL_GC = 2, ECL_MST = 3, ECL_SCC = 4, ECL_APSP = 5 } ecl_code;

@@ -31,11 +31,8 @@ typedef struct ecl_batch ecl_batch;
 #define ECL_BATCH_MST 0x8u
 #define ECL_BATCH_SCC 0x10u
 
-/* Runtime knobs the autotuner chooses (0 = built-in default). */
-typedef struct ecl_tune {
-  int32_t blocks_per_sm;      /* blocks of 256 threads per SM for the grid-stride kernels */
-  float mst_light_factor;     /* light-edge target, in multiples of n, for the MST filter */
-} ecl_tune;
+/* The engine's launch knobs are an ecl_tune (ecl_b200.h); ecl_batch_tune
+ * chooses them for the built batch. */
 
 ecl_status ecl_batch_create(ecl_batch** out);
 void ecl_batch_destroy(ecl_batch* b);

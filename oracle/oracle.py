@@ -160,3 +160,72 @@ def omp_gc(g) -> np.ndarray:
 
 def omp_scc(g) -> np.ndarray:
     return _omp("omp_scc", g, np.int32)
+
+
+# ---- seeded generators (gen.c): the benchmark graphs without the product library ----
+
+
+class _GenGraph(C.Structure):
+    _fields_ = [("nodes", C.c_int32), ("edges", C.c_int32), ("nindex", C.POINTER(C.c_int32)),
+                ("nlist", C.POINTER(C.c_int32)), ("eweight", C.POINTER(C.c_int32))]
+
+
+class Graph:
+    """CSR arrays with the attribute names the oracle functions read."""
+
+    def __init__(self, nindex, nlist, eweight=None, symmetric=False):
+        self.nindex = np.ascontiguousarray(nindex, dtype=np.int32)
+        self.nlist = np.ascontiguousarray(nlist, dtype=np.int32)
+        self.eweight = None if eweight is None else np.ascontiguousarray(eweight, dtype=np.int32)
+        self.symmetric = symmetric
+
+    @property
+    def nodes(self) -> int:
+        return int(self.nindex.shape[0] - 1)
+
+    @property
+    def edges(self) -> int:
+        return int(self.nlist.shape[0])
+
+
+_lib.gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.c_int32,
+                          C.c_uint64, C.c_int32, C.POINTER(_GenGraph)]
+_lib.gen_grid.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.c_uint64, C.c_int32, C.POINTER(_GenGraph)]
+_lib.gen_er.argtypes = [C.c_int32, C.c_double, C.c_uint64, C.c_int32, C.c_uint64, C.c_int32, C.c_int32,
+                        C.POINTER(_GenGraph)]
+_lib.gen_free.argtypes = [C.POINTER(_GenGraph)]
+for _f in (_lib.gen_rmat, _lib.gen_grid, _lib.gen_er):
+    _f.restype = C.c_int
+_lib.gen_free.restype = None
+
+
+def _gen_take(rc, g, symmetric, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with status {rc}")
+    try:
+        n, m = g.nodes, g.edges
+        nindex = np.ctypeslib.as_array(g.nindex, shape=(n + 1,)).copy()
+        nlist = np.ctypeslib.as_array(g.nlist, shape=(m,)).copy() if m else np.zeros(0, np.int32)
+        ew = np.ctypeslib.as_array(g.eweight, shape=(m,)).copy() if (g.eweight and m) else None
+    finally:
+        _lib.gen_free(C.byref(g))
+    return Graph(nindex, nlist, ew, symmetric)
+
+
+def gen_rmat(scale, edge_factor=16, a=0.57, b=0.19, c=0.19, seed=2, symmetrise=True, weight_seed=0,
+             weight_max=1 << 20) -> Graph:
+    g = _GenGraph()
+    rc = _lib.gen_rmat(scale, edge_factor, a, b, c, seed, int(symmetrise), weight_seed, weight_max, C.byref(g))
+    return _gen_take(rc, g, symmetrise, "gen_rmat")
+
+
+def gen_grid(rows, cols, delete_frac=0.05, seed=1, weight_seed=0, weight_max=1 << 20) -> Graph:
+    g = _GenGraph()
+    rc = _lib.gen_grid(rows, cols, delete_frac, seed, weight_seed, weight_max, C.byref(g))
+    return _gen_take(rc, g, True, "gen_grid")
+
+
+def gen_er(n, p, seed=4, symmetrise=False, weight_seed=0, weight_min=1, weight_max=1000) -> Graph:
+    g = _GenGraph()
+    rc = _lib.gen_er(n, p, seed, int(symmetrise), weight_seed, weight_min, weight_max, C.byref(g))
+    return _gen_take(rc, g, symmetrise, "gen_er")

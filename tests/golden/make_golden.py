@@ -9,97 +9,24 @@ reference produced on it:
   apsp                : the reference's CPU routine FW_cpu (ECL-APSP-atomic.cu:533).
 
 Usage (on a machine with a B200 and the built oracle/_ref library):
-    python tests/golden/make_golden.py OUTDIR
+    python tests/golden/make_golden.py OUTDIR [NAME ...]
 The fixtures in tests/golden/ were made this way and then copied there.
 """
-import ctypes as C
 import os
 import sys
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-sys.path[:0] = [os.path.join(ROOT, "ecl-suite_b200"), os.path.join(ROOT, "tests")]
+sys.path[:0] = [os.path.join(ROOT, "ecl-suite_b200"), os.path.join(ROOT, "tests"), os.path.join(ROOT, "oracle")]
 
 import ecl_b200 as ecl  # noqa: E402  (generators only)
 from conftest import from_edges, undirected  # noqa: E402
 
-REF = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libeclref.so"))
-REF.eclref_cc_device.restype = C.c_float
-REF.eclref_mis_device.restype = C.c_float
-REF.eclref_gc_device.restype = C.c_float
-REF.eclref_gc_scratch_bytes.restype = C.c_size_t
-REF.eclref_scc_device.restype = C.c_float
-REF.eclref_scc_scratch_bytes.restype = C.c_size_t
-REF.eclref_mst_cpu.restype = C.c_double
-REF.eclref_apsp_cpu.restype = C.c_double
+import refbuild  # noqa: E402  (the reference's own build, oracle/_ref)
 
-
-def P(a):
-    return C.c_void_p(a.ctypes.data if hasattr(a, "ctypes") else a.data_ptr())
-
-
-def dev(a):
-    import torch
-
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
-
-
-def ref_cc(g):
-    import torch
-
-    ni, nl = dev(g.nindex), dev(g.nlist if g.edges else np.zeros(1, np.int32))
-    st = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
-    wl = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
-    REF.eclref_cc_device(g.nodes, C.c_void_p(ni.data_ptr()), C.c_void_p(nl.data_ptr()), C.c_void_p(st.data_ptr()),
-                         C.c_void_p(wl.data_ptr()))
-    return st.cpu().numpy()
-
-
-def ref_mis(g):
-    import torch
-
-    ni, nl = dev(g.nindex), dev(g.nlist if g.edges else np.zeros(1, np.int32))
-    st = torch.empty((g.nodes + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
-    REF.eclref_mis_device(g.nodes, g.edges, C.c_void_p(ni.data_ptr()), C.c_void_p(nl.data_ptr()),
-                          C.c_void_p(st.data_ptr()))
-    return st.cpu().numpy()[: g.nodes]
-
-
-def ref_gc(g):
-    import torch
-
-    ni, nl = dev(g.nindex), dev(g.nlist if g.edges else np.zeros(1, np.int32))
-    col = torch.empty(g.nodes, dtype=torch.int32, device="cuda")
-    scr = torch.empty(REF.eclref_gc_scratch_bytes(g.nodes, g.edges) // 4 + 1, dtype=torch.int32, device="cuda")
-    REF.eclref_gc_device(g.nodes, g.edges, C.c_void_p(ni.data_ptr()), C.c_void_p(nl.data_ptr()),
-                         C.c_void_p(col.data_ptr()), C.c_void_p(scr.data_ptr()))
-    return col.cpu().numpy()
-
-
-def ref_scc(g):
-    import torch
-
-    ni, nl = dev(g.nindex), dev(g.nlist if g.edges else np.zeros(1, np.int32))
-    scr = torch.empty(REF.eclref_scc_scratch_bytes(g.nodes, g.edges) // 8 + 2, dtype=torch.int64, device="cuda")
-    lab = np.empty(g.nodes, np.int32)
-    REF.eclref_scc_device(g.nodes, g.edges, C.c_void_p(ni.data_ptr()), C.c_void_p(nl.data_ptr()), P(lab),
-                          C.c_void_p(scr.data_ptr()))
-    return lab
-
-
-def ref_mst(g):
-    out = np.zeros(max(g.edges, 1), np.uint8)
-    REF.eclref_mst_cpu(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), P(out))
-    out = out[: g.edges]
-    src = np.repeat(np.arange(g.nodes), np.diff(g.nindex))
-    return out, int(g.eweight[out.astype(bool)].astype(np.int64).sum()) if g.edges else 0
-
-
-def ref_apsp(g):
-    out = np.zeros((g.nodes, g.nodes), np.int32)
-    REF.eclref_apsp_cpu(g.nodes, g.edges, P(g.nindex), P(g.nlist), P(g.eweight), P(out))
-    return out
+ref_cc, ref_mis, ref_gc, ref_scc, ref_mst, ref_apsp = (refbuild.cc, refbuild.mis, refbuild.gc, refbuild.scc,
+                                                       refbuild.mst_cpu, refbuild.apsp_cpu)
 
 
 def pair_weights(g, seed):
@@ -134,12 +61,19 @@ def cases():
     yield "apsp_dups", "apsp", from_edges(4, [(0, 1), (0, 1), (1, 2), (2, 3), (0, 0), (3, 0)], weights=[9, 5, 2, 7, 3, 1])
     yield "apsp_er130", "apsp", ecl.gen_er(130, 0.03, seed=4, weight_seed=5)
     yield "apsp_er200", "apsp", ecl.gen_er(200, 0.02, seed=6, weight_seed=7)
+    # more than 64 colours: the reference's runLarge keeps the candidate
+    # colours of rows with 32 or more higher-priority entries in posscol2
+    # bitmaps (ECL-GC-atomic.cu:144, 148-251), a path no smaller case reaches
+    yield "gc_clique150", "gc", undirected(150, [(i, j) for i in range(150) for j in range(i + 1, 150)])
+    yield "gc_rmat13_ef64", "gc", ecl.gen_rmat(13, 64, seed=2)
 
 
-def main(outdir):
+def main(outdir, only=()):
     os.makedirs(outdir, exist_ok=True)
     fn = {"cc": ref_cc, "mis": ref_mis, "gc": ref_gc, "scc": ref_scc, "mst": ref_mst, "apsp": ref_apsp}
     for name, code, g in cases():
+        if only and name not in only:
+            continue
         res = fn[code](g)
         arrs = dict(nindex=g.nindex, nlist=g.nlist, code=np.array(code))
         if g.eweight is not None:
@@ -153,4 +87,5 @@ def main(outdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)))
+    # make_golden.py [OUTDIR [NAME ...]]: every fixture, or only the named ones
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__)), tuple(sys.argv[2:]))

@@ -37,8 +37,8 @@ def test_batch_tune_keeps_results(ecl, orc):
     b = ecl.Batch()
     b.add_mix(12, n_min=500, n_max=5000, seed=9, weight_max=1 << 16)
     b.build(ecl.BATCH_CC | ecl.BATCH_MIS | ecl.BATCH_MST)
-    bps, light = b.tune(trials=1)
-    assert bps in (4, 8) and light in (0.75, 1.5, 3.0)
+    t = b.tune(trials=1)
+    assert t.blocks_per_sm in (4, 8) and t.mst_light_factor in (0.75, 1.5, 3.0)
     b.run()
     for i in range(b.graphs):
         g = b.graph(i)

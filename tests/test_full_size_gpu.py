@@ -8,11 +8,19 @@
 - APSP: ER n=8192.  An O(n^3) host closure would take hours, so
   32 random rows are checked exactly against Dijkstra from those sources.
 - Batch: the 4096-graph mix, 16 sampled graphs against the oracle.
+
+The same configs are also compared with the reference's OWN race-free CUDA
+build (oracle/_ref, the reference's .cu files compiled unchanged) on the same
+graphs: CC, MIS, GC and SCC labels against its kernels, the MST edge set and
+weight against its cpuMST, and the APSP distances against FW_gpu_64.
 """
 import numpy as np
 import pytest
 
+import refbuild
+
 pytestmark = pytest.mark.gpu
+needs_ref = pytest.mark.skipif(not refbuild.available(), reason="oracle/_ref not built (make -C oracle ref)")
 
 
 @pytest.fixture(scope="module")
@@ -77,3 +85,48 @@ def test_batch4096_sampled_graphs(ecl, orc):
         inm, tot = b.result(int(i), ecl.BATCH_MST)
         einm, etot = orc.mst(g)
         assert tot == etot and np.array_equal(inm, einm), i
+
+
+# ------------------------------------------------ against the reference's own build
+
+
+@needs_ref
+def test_grid_cc_equals_reference_kernel(ecl):
+    g = ecl.gen_grid(1024, 1024, 0.05, seed=1)
+    assert np.array_equal(ecl.cc(g.to_device("cuda")).cpu().numpy(), refbuild.cc(g))
+
+
+@needs_ref
+def test_rmat22_cc_mis_scc_equal_reference_kernels(ecl, rmat22):
+    sym, dirg, dsym, ddir = rmat22
+    assert np.array_equal(ecl.cc(dsym).cpu().numpy(), refbuild.cc(sym))
+    assert np.array_equal(ecl.mis(dsym).cpu().numpy(), refbuild.mis(sym))
+    assert np.array_equal(ecl.scc(ddir).cpu().numpy(), refbuild.scc(dirg))
+
+
+@needs_ref
+def test_rmat22_gc_equals_reference_kernels(ecl, rmat22):
+    """Bit-identical colours, hence the same colour count (the north-star bar
+    is "no more colours than the reference")."""
+    sym, _, dsym, _ = rmat22
+    got = ecl.gc(dsym).cpu().numpy()
+    ref = refbuild.gc(sym)
+    assert int(got.max()) <= int(ref.max())
+    assert np.array_equal(got, ref)
+
+
+@needs_ref
+def test_rmat22_mst_equals_reference_cpumst(ecl, rmat22):
+    sym, _, dsym, _ = rmat22
+    in_mst, total = ecl.mst(dsym)
+    ref_in, ref_total = refbuild.mst_cpu(sym)
+    assert total == ref_total
+    assert np.array_equal(in_mst.cpu().numpy(), ref_in)
+
+
+@needs_ref
+def test_apsp_er8192_equals_reference_fw_gpu_64(ecl):
+    g = ecl.gen_er(8192, 0.001, seed=4, weight_seed=5, weight_min=1, weight_max=1000)
+    dist = ecl.apsp(g.to_device("cuda")).cpu().numpy()
+    ref = refbuild.apsp_gpu(g)
+    assert np.array_equal(dist, ref[: g.nodes, : g.nodes])

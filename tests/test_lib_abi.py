@@ -25,7 +25,7 @@ def test_header_symbols_exported(ecl):
 
 
 def test_abi_version_and_status_strings(ecl):
-    assert ecl.lib.ecl_abi_version() == 1
+    assert ecl.lib.ecl_abi_version() == 2
     for s in range(9):
         assert ecl.lib.ecl_status_string(s)
     assert ecl.lib.ecl_status_string(999) == b"unknown status"
@@ -63,3 +63,19 @@ def test_bad_arguments_rejected_before_device(ecl):
     v = g.view()
     out = np.empty(1, np.int32)
     assert ecl.lib.ecl_cc(ctypes.byref(v), out.ctypes.data, ctypes.byref(o)) == ecl.ERR_BAD_GRAPH
+
+
+def test_tune_knobs_round_trip_and_range_checks(ecl):
+    """ecl_set_tune keeps valid knobs process-wide and rejects out-of-range
+    ones without changing anything (no device needed)."""
+    old = ecl.set_tune(gc_core_ranks=1024, blocks_per_sm=4)
+    try:
+        t = ecl.get_tune()
+        assert (t.gc_core_ranks, t.blocks_per_sm) == (1024, 4)
+        bad = ecl.Tune()
+        bad.gc_core_ranks = 1 << 20
+        assert ecl.lib.ecl_set_tune(ctypes.byref(bad)) == ecl.ERR_INVALID_ARG
+        assert ecl.get_tune().gc_core_ranks == 1024
+    finally:
+        ecl.set_tune(old)
+    assert ecl.get_tune().as_dict() == old.as_dict()

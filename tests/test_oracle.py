@@ -104,3 +104,26 @@ def test_apsp_rows_match_the_closure(orc, ecl):
     # duplicates: the last entry of an arc wins, as in the matrix fill
     d = from_edges(3, [(0, 1), (0, 1), (1, 2)], weights=[9, 4, 2])
     assert np.array_equal(orc.apsp_rows(d, np.array([0])), orc.apsp(d)[[0]])
+
+
+def test_oracle_generators_equal_the_library_generators(orc, ecl):
+    """The reference arm of the bench builds its graphs with the oracle's
+    restated generators (it must not load the product library); they give the
+    same CSR and weights byte for byte as ecl_gen_rmat / _grid / _er."""
+
+    def same(a, b):
+        if not (np.array_equal(a.nindex, b.nindex) and np.array_equal(a.nlist, b.nlist)):
+            return False
+        if a.eweight is None or b.eweight is None:
+            return a.eweight is None and b.eweight is None
+        return np.array_equal(a.eweight, b.eweight)
+
+    assert same(orc.gen_rmat(13, 16, seed=2, weight_seed=3), ecl.gen_rmat(13, 16, seed=2, weight_seed=3))
+    assert same(orc.gen_rmat(12, 16, seed=2, symmetrise=False), ecl.gen_rmat(12, 16, seed=2, symmetrise=False))
+    assert same(orc.gen_rmat(11, 8, 0.45, 0.15, 0.15, seed=7), ecl.gen_rmat(11, 8, 0.45, 0.15, 0.15, seed=7))
+    assert same(orc.gen_grid(64, 48, 0.05, seed=1), ecl.gen_grid(64, 48, 0.05, seed=1))
+    assert same(orc.gen_grid(30, 20, 0.3, seed=1, weight_seed=9, weight_max=1 << 16),
+                ecl.gen_grid(30, 20, 0.3, seed=1, weight_seed=9, weight_max=1 << 16))
+    assert same(orc.gen_er(2000, 0.004, seed=4, weight_seed=5), ecl.gen_er(2000, 0.004, seed=4, weight_seed=5))
+    assert same(orc.gen_er(2000, 0.004, seed=4, symmetrise=True, weight_seed=5),
+                ecl.gen_er(2000, 0.004, seed=4, symmetrise=True, weight_seed=5))

@@ -85,6 +85,24 @@ def test_gc_large_colour_windows(ecl, orc):
 # ------------------------------------------------------------------------- MST
 
 
+@pytest.mark.parametrize("core", [1, 7, 64, 0])
+def test_gc_core_size_does_not_change_colours(ecl, orc, core):
+    """The leading ranks are coloured in one CTA's shared memory and the rest
+    by the grid-wide pull; where the boundary lies (1, 7, 64 ranks, or the
+    default, which covers every long row of these graphs) changes no colour.
+    A 2100-clique forces colours past the first 2048-colour window inside the
+    core."""
+    old = ecl.set_tune(gc_core_ranks=core)
+    try:
+        cases = list(sym_cases(ecl)) + [("rmat16", ecl.gen_rmat(16, 16, seed=3))]
+        if core == 0:
+            cases.append(("clique2100", undirected(2100, [(i, j) for i in range(2100) for j in range(i + 1, 2100)])))
+        for name, g in cases:
+            assert np.array_equal(ecl.gc(g), orc.gc(g)), (core, name)
+    finally:
+        ecl.set_tune(old)
+
+
 def test_gc_short_row_ignores_colours_above_its_range(ecl, orc):
     """A row of <= 32 entries (one lane) whose higher neighbour is a hub with
     colour 64 or more: that colour cannot be its smallest free one and must
