@@ -240,8 +240,11 @@ def phase_bytes(code, phase, n, m):
         ("mis", 0): 4 * (n + 1) + n,
         ("mis", 1): csr + n,
         ("mis", 2): 2 * n,
-        ("gc", 0): csr + 4 * (m // 2) + 4 * n,     # init: CSR read, higher-priority half of nl2 + counts written
-        ("gc", 1): 7 * 24 * n,                     # keys + 7 radix passes over (8 B key, 4 B value), read + write
+        # keys + init: rows read for the keys (4n), keys + ids written (12n), CSR read once, the
+        # higher-priority half of nl2 and the counts written
+        ("gc", 0): csr + 16 * n + 4 * (m // 2) + 4 * n,
+        # radix passes over (8 B key, 4 B value), read + write; 32 hash bits + the bits of m
+        ("gc", 1): -(-(32 + max(1, m.bit_length())) // 8) * 24 * n,
         ("gc", 2): None,                           # core: latency-bound, no byte model (its entries are booked to pull)
         ("gc", 3): 4 * (n + 1) + 4 * (m // 2) + 12 * n,  # pull: higher-priority half read once, order, colours
         ("mst", 0): 16 * n,
@@ -260,7 +263,7 @@ PHASE_NAMES = {
     "cc": ["cc_init", "cc_hook", "cc_chunks", "cc_flatten"],
     "cc_sym": ["cc_init+sample+giant", "cc_rest", "cc_rest_chunks", "cc_flatten"],
     "mis": ["mis_init", "mis_run", "mis_emit"],
-    "gc": ["gc_init+chunks", "gc_keys+radix_sort", "gc_core", "gc_pull"],
+    "gc": ["gc_keys+init+chunks", "radix_sort", "gc_core", "gc_pull"],
     "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
             "mst_boruvka(heavy)"],
     "scc": ["scc_mark+chunks", "scc_build+chunks", "scc_solve"],
@@ -363,7 +366,7 @@ def bench_batch(args, rank, world, local_rank):
                    "codes": "CC+MIS+MST", "parallelism": f"replicas x{world}"},
         "plain_graphs_per_s": plain_gps, "plain_ms": plain_ms, "speedup_vs_plain": value / plain_gps,
         "edges_per_s": 3 * tot_m * args.steps / (ms / 1e3),
-        "cuda_graph_replay": replay, "tuned": tuned.as_dict(),
+        "cuda_graph_replay": replay, "tuned": tuned.as_dict(), "tune_points": b.tune_points,
         "setup_s": {"generate": round(gen_s, 2), "build_upload": round(build_s, 2), "tune": round(tune_s, 2)},
         "gpu_launches": int(launches), "clocks": clocks,
     }

@@ -78,6 +78,7 @@ struct ecl_batch {
   cudaStream_t stream = nullptr;  // the engine's own non-blocking stream (runs + capture)
   ecl::DeviceInfo dev;
   ecl_tune tune{};
+  int32_t tune_points = 0;  // knob settings the last ecl_batch_tune timed
   std::vector<void*> allocs;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -395,37 +396,69 @@ ecl_status ecl_batch_set_tune(ecl_batch* b, const ecl_tune* t) {
   return ECL_OK;
 }
 
+// The autotuner: coordinate descent over the launch knobs on the built batch.
+// Starting from the defaults, each knob in turn takes every candidate value
+// (the others held at the best point so far) and keeps the fastest; a point
+// costs one capturing run plus `trials` timed replays.  The knobs are the
+// ones the reference fixes at compile time -- grid size, the per-lane / per-
+// warp / chunk row thresholds (ECL-CC-atomic.cu:62,120,122; ECL-MST_10-
+// atomic.cu:197), the MST light/heavy split (ECL-MST_10-atomic.cu:450-459)
+// and, with GC in the batch, the size of GC's shared-memory core.
 ecl_status ecl_batch_tune(ecl_batch* b, int32_t trials, ecl_tune* best) {
   using namespace ecl;
   if (!b || !b->built || trials < 1) return ECL_ERR_INVALID_ARG;
-  const int bps[] = {4, 8};
-  const float light[] = {0.75f, 1.5f, 3.0f};
-  ecl_tune winner{};
-  float best_ms = 1e30f;
-  for (int x : bps) {
-    for (float l : light) {
-      ecl_tune t;
-      t.blocks_per_sm = x;
-      t.mst_light_factor = (b->codes & ECL_BATCH_MST) ? l : 0.f;
-      ecl_status st = ecl_batch_set_tune(b, &t);
+  auto time_point = [&](const ecl_tune& t, float* ms) -> ecl_status {
+    ecl_status st = ecl_batch_set_tune(b, &t);
+    if (st != ECL_OK) return st;
+    float tot = 0.f;
+    for (int r = 0; r < trials + 1; r++) {  // the first run captures
+      ecl_opts o{};
+      st = ecl_batch_run(b, &o);
       if (st != ECL_OK) return st;
-      float tot = 0.f;
-      for (int r = 0; r < trials + 1; r++) {  // first run captures
-        ecl_opts o{};
-        st = ecl_batch_run(b, &o);
-        if (st != ECL_OK) return st;
-        if (r > 0) tot += o.elapsed_ms;
-      }
-      if (tot < best_ms) {
-        best_ms = tot;
+      if (r > 0) tot += o.elapsed_ms;
+    }
+    *ms = tot;
+    return ECL_OK;
+  };
+  struct Knob {
+    bool active;
+    std::vector<float> values;
+    void (*set)(ecl_tune&, float);
+  };
+  const std::vector<Knob> knobs = {
+      {true, {8.f, 4.f, 6.f}, [](ecl_tune& t, float v) { t.blocks_per_sm = (int32_t)v; }},
+      {(b->codes & ECL_BATCH_MST) != 0, {0.75f, 1.5f, 3.f, 0.4f}, [](ecl_tune& t, float v) { t.mst_light_factor = v; }},
+      {true, {32.f, 16.f, 8.f}, [](ecl_tune& t, float v) { t.row_lane_max = (int32_t)v; }},
+      {true, {256.f, 128.f, 512.f, 2048.f}, [](ecl_tune& t, float v) { t.row_chunk = (int32_t)v; }},
+      {(b->codes & ECL_BATCH_GC) != 0, {32768.f, 8192.f, 1024.f}, [](ecl_tune& t, float v) { t.gc_core_ranks = (int32_t)v; }},
+  };
+  ecl_tune winner{};
+  for (const Knob& k : knobs)
+    if (k.active) k.set(winner, k.values[0]);
+  float best_ms = 0.f;
+  ecl_status st = time_point(winner, &best_ms);
+  if (st != ECL_OK) return st;
+  b->tune_points = 1;
+  for (const Knob& k : knobs) {
+    if (!k.active) continue;
+    for (size_t i = 1; i < k.values.size(); i++) {
+      ecl_tune t = winner;
+      k.set(t, k.values[i]);
+      float ms = 0.f;
+      st = time_point(t, &ms);
+      if (st != ECL_OK) return st;
+      b->tune_points++;
+      if (ms < best_ms) {
+        best_ms = ms;
         winner = t;
       }
-      if (!(b->codes & ECL_BATCH_MST)) break;
     }
   }
   if (best) *best = winner;
   return ecl_batch_set_tune(b, &winner);
 }
+
+int32_t ecl_batch_tune_points(const ecl_batch* b) { return b ? b->tune_points : 0; }
 
 int32_t ecl_batch_graphs(const ecl_batch* b) { return b ? (int32_t)b->graphs.size() : 0; }
 int32_t ecl_batch_superbatches(const ecl_batch* b) { return b ? (int32_t)b->sup.size() : 0; }

@@ -15,9 +15,10 @@
 //                kInitScan entries (one free hook per vertex).
 //  * cc_hook   - one pass over the vertices, 32 per warp.  Lists of <= 16
 //                entries are walked by their own lane; lists of up to
-//                kChunk entries are walked by the whole warp (ballot loop,
+//                2048 entries are walked by the whole warp (ballot loop,
 //                coalesced 128-byte nlist reads); longer lists are cut into
-//                kChunk-entry chunk records for cc_chunks.
+//                2048-entry chunk records for cc_chunks (both thresholds
+//                are launch knobs).
 //  * cc_chunks - warp per chunk record, so a 163k-entry R-MAT hub is spread
 //                over ~160 warps instead of serialising one block.
 //  * cc_flatten- label[v] = root(v).
@@ -33,8 +34,9 @@ namespace {
 using namespace dev;
 
 constexpr int kTPB = 256;
-constexpr int kLaneMax = 16;   // lists up to this length: lane-level
-constexpr int kChunk = 2048;   // lists longer than this: chunk records
+// Default degree bins: lists of <= 16 entries per lane, chunk records of
+// 2048 entries (a launch knob may change both).
+constexpr Bins kCCBins{16, 2048};
 constexpr int kInitScan = 8;   // entries cc_init looks at for a first smaller neighbour
 
 // Row [beg, end) of v, or empty when the row is malformed (cc_init reports it).
@@ -143,19 +145,20 @@ __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restr
   }
 }
 
-// Chunk records of chunk_capacity(m) cover every long row of a CSR whose rows
-// do not overlap (a row of d > kChunk entries needs ceil(d / kChunk) <
-// 2 d / kChunk records).  A malformed CSR with overlapping rows can ask for
-// more: the excess raises ECL_ERR_BAD_GRAPH and is not written.
-constexpr int chunk_capacity(int m) { return 2 * (m / kChunk) + 2; }
+// Chunk records of chunk_capacity(m, chunk) cover every long row of a CSR
+// whose rows do not overlap (a row of d > chunk entries needs
+// ceil(d / chunk) < 2 d / chunk records).  A malformed CSR with overlapping
+// rows can ask for more: the excess raises ECL_ERR_BAD_GRAPH and is not
+// written.
+constexpr int chunk_capacity(int m, int chunk) { return 2 * (m / chunk) + 2; }
 
-__device__ __forceinline__ void cc_push_chunks(int v, int beg, int deg, int2* chunks, int cap, CCCounters* ctr,
-                                               Status* status) {
-  const int nc = (deg + kChunk - 1) / kChunk;
+__device__ __forceinline__ void cc_push_chunks(int v, int beg, int deg, int chunk, int2* chunks, int cap,
+                                               CCCounters* ctr, Status* status) {
+  const int nc = (deg + chunk - 1) / chunk;
   const int at = fetch_add(&ctr->nchunks, nc);
   for (int c = 0; c < nc; c++) {
     if ((unsigned)(at + c) < (unsigned)cap)
-      chunks[at + c] = make_int2(v, beg + c * kChunk);
+      chunks[at + c] = make_int2(v, beg + c * chunk);
     else
       raise(status, ECL_ERR_BAD_GRAPH, v);
   }
@@ -169,8 +172,8 @@ __device__ __forceinline__ int cc_chunk_total(const CCCounters* ctr, int cap) {
 
 __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ parent,
-                                                int2* __restrict__ chunks, int chunk_cap, CCCounters* __restrict__ ctr,
-                                                Status* __restrict__ status) {
+                                                int2* __restrict__ chunks, int chunk_cap, Bins bins,
+                                                CCCounters* __restrict__ ctr, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -179,9 +182,9 @@ __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restr
     int beg = 0, end = 0;
     if (v < n) cc_row(nindex, v, m, beg, end);
     const int deg = end - beg;
-    if (deg > kChunk) {
-      cc_push_chunks(v, beg, deg, chunks, chunk_cap, ctr, status);
-    } else if (deg > 0 && deg <= kLaneMax) {
+    if (deg > bins.chunk) {
+      cc_push_chunks(v, beg, deg, bins.chunk, chunks, chunk_cap, ctr, status);
+    } else if (deg > 0 && deg <= bins.lane) {
       int rv = -1;
       for (int i = beg; i < end; i++) {
         const int u = __ldg(&nlist[i]);
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restr
       }
     }
     // Medium lists: the whole warp walks one list at a time.
-    unsigned mid = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
+    unsigned mid = __ballot_sync(kFull, deg > bins.lane && deg <= bins.chunk);
     while (mid) {
       const int who = __ffs(mid) - 1;
       mid &= mid - 1;
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__(kTPB) cc_hook(int n, int m, const int* __restr
 
 __global__ void __launch_bounds__(kTPB) cc_chunks(int n, const int* __restrict__ nindex,
                                                   const int* __restrict__ nlist, int* __restrict__ parent,
-                                                  const int2* __restrict__ chunks, int chunk_cap,
+                                                  const int2* __restrict__ chunks, int chunk_cap, int chunk,
                                                   const CCCounters* __restrict__ ctr, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(kTPB) cc_chunks(int n, const int* __restrict__
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
-    const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
+    const int end = min(rec.y + chunk, __ldg(&nindex[v + 1]));
     int rv = -1;
     for (int i = rec.y + lane; i < end; i += 32) {
       const int u = __ldg(&nlist[i]);
@@ -346,7 +349,7 @@ __device__ __forceinline__ bool cc_rest_wanted(int u, int v, const unsigned char
 __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ parent,
                                                 const unsigned char* __restrict__ ing, int2* __restrict__ chunks,
-                                                int chunk_cap, CCCounters* __restrict__ ctr,
+                                                int chunk_cap, Bins bins, CCCounters* __restrict__ ctr,
                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -359,9 +362,9 @@ __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restr
       beg = min(end, beg + kSample);  // the first entries were linked by cc_sample
     }
     const int deg = end - beg;
-    if (deg > kChunk) {
-      cc_push_chunks(v, beg, deg, chunks, chunk_cap, ctr, status);
-    } else if (deg > 0 && deg <= kLaneMax) {
+    if (deg > bins.chunk) {
+      cc_push_chunks(v, beg, deg, bins.chunk, chunks, chunk_cap, ctr, status);
+    } else if (deg > 0 && deg <= bins.lane) {
       int rv = -1;
       for (int i = beg; i < end; i++) {
         const int u = __ldg(&nlist[i]);
@@ -372,7 +375,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restr
         }
       }
     }
-    unsigned mid = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
+    unsigned mid = __ballot_sync(kFull, deg > bins.lane && deg <= bins.chunk);
     while (mid) {
       const int who = __ffs(mid) - 1;
       mid &= mid - 1;
@@ -395,7 +398,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest(int n, int m, const int* __restr
 __global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ parent,
                                                        const unsigned char* __restrict__ ing,
-                                                       const int2* __restrict__ chunks, int chunk_cap,
+                                                       const int2* __restrict__ chunks, int chunk_cap, int chunk,
                                                        const CCCounters* __restrict__ ctr, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restr
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
-    const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
+    const int end = min(rec.y + chunk, __ldg(&nindex[v + 1]));
     int rv = -1;
     for (int i = rec.y + lane; i < end; i += 32) {
       const int u = __ldg(&nlist[i]);
@@ -419,7 +422,7 @@ __global__ void __launch_bounds__(kTPB) cc_rest_chunks(int n, const int* __restr
 
 void cc_layout(Carve& c, int n, int m, CCCounters** ctr, int2** chunks, unsigned char** ing = nullptr) {
   *ctr = c.take<CCCounters>(1);
-  *chunks = c.take<int2>((size_t)chunk_capacity(m));
+  *chunks = c.take<int2>((size_t)chunk_capacity(m, kMinChunk));
   unsigned char* g = c.take<unsigned char>((size_t)n);
   if (ing) *ing = g;
 }
@@ -446,6 +449,8 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   unsigned char* ing;
   cc_layout(c, g.n, g.m, &ctr, &chunks, &ing);
   const int grid = dev.grid_blocks(kTPB);
+  const Bins bins = bins_of(dev, kCCBins);
+  const int cap = chunk_capacity(g.m, kMinChunk);  // cc_layout sized the records for the smallest chunk
   ECL_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(CCCounters), stream));
   if (g.flags & ECL_GRAPH_SYMMETRIC) {
     ECL_LAUNCH(cc_init<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
@@ -456,11 +461,11 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
     ECL_LAUNCH(cc_giant, 1, 1024, 0, stream, g.n, parent, ctr);
     ECL_LAUNCH(cc_mark_giant, grid, kTPB, 0, stream, g.n, parent, ctr, ing);
     mark();
-    ECL_LAUNCH(cc_rest, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, ing, chunks, chunk_capacity(g.m), ctr,
+    ECL_LAUNCH(cc_rest, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, ing, chunks, cap, bins, ctr,
                status);
     mark();
-    ECL_LAUNCH(cc_rest_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, ing, chunks, chunk_capacity(g.m), ctr,
-               status);
+    ECL_LAUNCH(cc_rest_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, ing, chunks, cap, bins.chunk,
+               ctr, status);
     mark();
     ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
     mark();
@@ -468,11 +473,9 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   }
   ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, status);
   mark();
-  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, chunk_capacity(g.m), ctr,
-             status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, parent, chunks, cap, bins, ctr, status);
   mark();
-  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, chunks, chunk_capacity(g.m), ctr,
-             status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, parent, chunks, cap, bins.chunk, ctr, status);
   mark();
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, g.n, parent);
   mark();
@@ -520,7 +523,10 @@ namespace ecl {
 namespace {
 
 constexpr size_t kNoAllocBytes = ECL_CC_NOALLOC_SCRATCH_BYTES;
-static_assert(kStatusBytes + sizeof(CCCounters) + 256 + sizeof(int2) * (size_t)chunk_capacity(ECL_CC_NOALLOC_MAX_EDGES) <=
+// The allocation-free path always uses the default bins (no knob may enlarge
+// its fixed array), so its records are sized for kCCBins.chunk.
+static_assert(kStatusBytes + sizeof(CCCounters) + 256 +
+                      sizeof(int2) * (size_t)chunk_capacity(ECL_CC_NOALLOC_MAX_EDGES, kCCBins.chunk) <=
                   kNoAllocBytes,
               "no-alloc scratch too small for ECL_CC_NOALLOC_MAX_EDGES");
 
@@ -605,10 +611,10 @@ extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t
   ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
   const int grid = dev.grid_blocks(kTPB);
   ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
-  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks, chunk_capacity(edges), ctr,
-             status);
-  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks, chunk_capacity(edges), ctr,
-             status);
+  ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks,
+             chunk_capacity(edges, kCCBins.chunk), kCCBins, ctr, status);
+  ECL_LAUNCH(cc_chunks, grid, kTPB, 0, stream, nodes, nindex, nlist, label, chunks,
+             chunk_capacity(edges, kCCBins.chunk), kCCBins.chunk, ctr, status);
   ECL_LAUNCH(cc_flatten, grid, kTPB, 0, stream, nodes, label);
   Status hs{};
   ECL_CUDA_TRY(cudaMemcpyAsync(&hs, status, sizeof(hs), cudaMemcpyDeviceToHost, stream));

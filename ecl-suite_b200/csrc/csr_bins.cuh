@@ -1,12 +1,14 @@
 // Degree binning shared by the CSR scans.
 //
-// A row of <= kBinLane entries is walked by its own lane, all lanes of the
+// A row of <= bins.lane entries is walked by its own lane, all lanes of the
 // warp stepping through entry offset k together (so warp-aggregated appends
-// stay converged); a row of <= kBinChunk entries by the whole warp, 32
-// entries per step; a longer row is cut into kBinChunk-entry chunk records
+// stay converged); a row of <= bins.chunk entries by the whole warp, 32
+// entries per step; a longer row is cut into bins.chunk-entry chunk records
 // that a second launch spreads over all warps.  R-MAT puts its heaviest rows
 // at the lowest ids, i.e. in the same warp groups, so the chunk size -- not
-// the lane/warp split -- bounds the work of the slowest warp.
+// the lane/warp split -- bounds the work of the slowest warp.  Both
+// thresholds are launch knobs (ecl_tune): each scan has its own default, and
+// the results never depend on them.
 #pragma once
 
 #include "common.cuh"
@@ -17,6 +19,14 @@ namespace dev {
 
 constexpr int kBinLane = 32;
 constexpr int kBinChunk = 256;
+// Smallest chunk a knob may ask for: workspaces hold chunk records for it.
+constexpr int kMinChunk = 128;
+constexpr int kMaxChunk = 8192;
+
+struct Bins {
+  int lane;   // rows of at most this many entries: one lane (1..32)
+  int chunk;  // rows longer than this: chunk records of this many entries (power of two)
+};
 
 // Chunk records of the long rows.  `cap` records fit: 2 * (m / chunk) + 2
 // covers every row of a CSR whose rows do not overlap (each long row of d
@@ -49,17 +59,16 @@ __device__ __forceinline__ void csr_row(const int* nindex, int v, int m, int& be
 }
 
 // Chunk records for the long rows of a warp's 32 vertices: every lane of the
-// warp calls; lanes with `is_long` cut [beg, end) into kChunkLen-entry
-// records (vertex, first entry).  One atomic per warp reserves all of them
+// warp calls; lanes with `is_long` cut [beg, end) into `chunk`-entry records
+// (vertex, first entry).  One atomic per warp reserves all of them
 // (R-MAT-22 has ~50k rows over 256 entries; an atomic per row on one counter
 // would serialise in L2); the records land in lane order.  Records past the
 // capacity (only a CSR with overlapping rows asks for them) raise
 // ECL_ERR_BAD_GRAPH and are dropped.
-template <int kChunkLen>
-__device__ __forceinline__ void push_chunks_warp(const RowChunks& rc, bool is_long, int v, int beg, int end,
+__device__ __forceinline__ void push_chunks_warp(const RowChunks& rc, int chunk, bool is_long, int v, int beg, int end,
                                                  Status* status) {
   const int lane = threadIdx.x & 31;
-  const int nc = is_long ? (end - beg + kChunkLen - 1) / kChunkLen : 0;
+  const int nc = is_long ? (end - beg + chunk - 1) / chunk : 0;
   if (!__any_sync(kFull, nc > 0)) return;
   int incl = nc;  // inclusive prefix sum over the warp
 #pragma unroll
@@ -73,7 +82,7 @@ __device__ __forceinline__ void push_chunks_warp(const RowChunks& rc, bool is_lo
   base = __shfl_sync(kFull, base, 0) + incl - nc;
   for (int c = 0; c < nc; c++) {
     if ((unsigned)(base + c) < (unsigned)rc.cap)  // a wrapped counter stays out too
-      rc.rec[base + c] = make_int2(v, beg + c * kChunkLen);
+      rc.rec[base + c] = make_int2(v, beg + c * chunk);
     else
       raise(status, ECL_ERR_BAD_GRAPH, v);
   }

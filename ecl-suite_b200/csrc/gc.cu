@@ -8,12 +8,14 @@
 // never higher priority (:102 compares v with itself) and are ignored.
 //
 // B200 design: greedy colouring pulled in priority order.
-//  * gc_init / gc_init_chunks (degree-binned: lane / warp / 256-entry chunk
-//    records) compact every row's higher-priority entries to the front of
-//    the row's slot in nl2[]; hc[v] = their number.
-//  * gc_keys + radix_sort_pairs rank all vertices by priority (a stable LSD
-//    sort on the inverted (degree, hash) key over ids in descending order),
-//    which is a topological order of the colouring dependencies.
+//  * gc_keys writes every vertex's priority key (the inverted (degree, hash)
+//    word); gc_init / gc_init_chunks (degree-binned: lane / warp / 256-entry
+//    chunk records) compare each list entry with one 8-byte key load and
+//    compact every row's higher-priority entries to the front of the row's
+//    slot in nl2[]; hc[v] = their number.
+//  * radix_sort_pairs then ranks all vertices by priority (a stable LSD sort
+//    of those keys over ids in descending order), which is a topological
+//    order of the colouring dependencies.
 //  * gc_pull is ONE cooperative persistent launch.  Ranks are dealt to the
 //    warps round-robin -- one long row (> 32 entries; they form a prefix of
 //    the order, priority being degree-first) or 32 short rows at a time --
@@ -54,12 +56,6 @@ struct GCCtl {
   int pad2[30];
 };
 
-__device__ __forceinline__ bool gc_outranks(int du, unsigned hu, int u, int dv, unsigned hv, int v) {
-  if (du != dv) return du > dv;
-  if (hu != hv) return hu > hv;
-  return u > v;
-}
-
 // Priority hash of vertex x: the reference hashes the vertex id; in a union
 // of graphs (vhash != nullptr) it is the hash of x's LOCAL id, precomputed.
 __device__ __forceinline__ unsigned gc_h(const unsigned* vhash, int x) {
@@ -70,17 +66,19 @@ __device__ __forceinline__ unsigned gc_h(const unsigned* vhash, int x) {
 constexpr int kInitBatch = 4;
 
 // Classes of kInitBatch list entries of v -- 0: ignore (self-loop or
-// invalid), 1: higher priority than v, 2: lower.  The list entries are loaded
-// first, then both row bounds of every neighbour, all before any is compared.
+// invalid), 1: higher priority than v, 2: lower.  A vertex's priority is its
+// sort key (gc_keys: the inverted (degree, hash) word, so a SMALLER key is a
+// higher priority) with ties to the larger id; kv is v's key.  The list
+// entries are loaded first, then every neighbour's key (one 8-byte load each
+// instead of both row bounds and a rehash), all before any is compared.
 __device__ __forceinline__ void gc_class_batch(const int (&u)[kInitBatch], const bool (&valid)[kInitBatch], int v,
-                                               int dv, unsigned hv, int n, const int* nindex, const unsigned* vhash,
+                                               unsigned long long kv, int n, const unsigned long long* keys,
                                                Status* status, int (&cls)[kInitBatch]) {
-  int b[kInitBatch], e[kInitBatch];
+  unsigned long long ku[kInitBatch];
 #pragma unroll
   for (int k = 0; k < kInitBatch; k++) {
     const bool ok = valid[k] && (unsigned)u[k] < (unsigned)n && u[k] != v;
-    b[k] = ok ? __ldg(&nindex[u[k]]) : 0;
-    e[k] = ok ? __ldg(&nindex[u[k] + 1]) : 0;
+    ku[k] = ok ? __ldg(&keys[n - 1 - u[k]]) : 0ull;
   }
 #pragma unroll
   for (int k = 0; k < kInitBatch; k++) {
@@ -89,7 +87,7 @@ __device__ __forceinline__ void gc_class_batch(const int (&u)[kInitBatch], const
     if ((unsigned)u[k] >= (unsigned)n) {
       raise(status, ECL_ERR_BAD_GRAPH, u[k]);
     } else if (u[k] != v) {
-      cls[k] = gc_outranks(e[k] - b[k], gc_h(vhash, u[k]), u[k], dv, hv, v) ? 1 : 2;
+      cls[k] = (ku[k] < kv || (ku[k] == kv && u[k] > v)) ? 1 : 2;
     }
   }
 }
@@ -110,7 +108,8 @@ __global__ void __launch_bounds__(kTPB) gc_union_hash(int n, const int* __restri
 
 __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ nl2,
-                                                int* __restrict__ hc, RowChunks rc, const unsigned* __restrict__ vhash,
+                                                int* __restrict__ hc, RowChunks rc, Bins bins,
+                                                const unsigned long long* __restrict__ keys,
                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -120,10 +119,10 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
     int beg = 0, end = 0;
     if (v < n) csr_row(nindex, v, m, beg, end, status);
     const int dv = end - beg;
-    const unsigned hv = (v < n) ? gc_h(vhash, v) : 0u;
+    const unsigned long long kv = (v < n) ? __ldg(&keys[n - 1 - v]) : 0ull;
     int h = 0;
-    push_chunks_warp<kBinChunk>(rc, dv > kBinChunk, v, beg, end, status);
-    if (v < n && dv <= kBinLane) {
+    push_chunks_warp(rc, bins.chunk, dv > bins.chunk, v, beg, end, status);
+    if (v < n && dv <= bins.lane) {
       for (int i0 = beg; i0 < end; i0 += kInitBatch) {
         int u[kInitBatch], cls[kInitBatch];
         bool valid[kInitBatch];
@@ -132,20 +131,20 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
           valid[k] = i0 + k < end;
           u[k] = valid[k] ? __ldg(&nlist[i0 + k]) : 0;
         }
-        gc_class_batch(u, valid, v, dv, hv, n, nindex, vhash, status, cls);
+        gc_class_batch(u, valid, v, kv, n, keys, status, cls);
 #pragma unroll
         for (int k = 0; k < kInitBatch; k++)
           if (cls[k] == 1) nl2[beg + h++] = u[k];
       }
     }
-    unsigned todo = __ballot_sync(kFull, dv > kBinLane && dv <= kBinChunk);
+    unsigned todo = __ballot_sync(kFull, dv > bins.lane && dv <= bins.chunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
       const int wv = __shfl_sync(kFull, v, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      const unsigned whv = gc_h(vhash, wv);
+      const unsigned long long wkv = __shfl_sync(kFull, kv, who);
       int wh = 0;
       for (int i0 = wbeg; i0 < wend; i0 += 32 * kInitBatch) {
         int u[kInitBatch], cls[kInitBatch];
@@ -155,7 +154,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
           valid[k] = i0 + 32 * k + lane < wend;
           u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
         }
-        gc_class_batch(u, valid, wv, wend - wbeg, whv, n, nindex, vhash, status, cls);
+        gc_class_batch(u, valid, wv, wkv, n, keys, status, cls);
 #pragma unroll
         for (int k = 0; k < kInitBatch; k++) {
           const unsigned bh = __ballot_sync(kFull, cls[k] == 1);
@@ -165,14 +164,14 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       }
       if (lane == who) h = wh;
     }
-    if (v < n) hc[v] = dv > kBinChunk ? 0 : h;  // chunked rows start at 0, counted by gc_init_chunks
+    if (v < n) hc[v] = dv > bins.chunk ? 0 : h;  // chunked rows start at 0, counted by gc_init_chunks
   }
 }
 
 __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ nl2,
-                                                       int* __restrict__ hc, RowChunks rc,
-                                                       const unsigned* __restrict__ vhash,
+                                                       int* __restrict__ hc, RowChunks rc, int chunk,
+                                                       const unsigned long long* __restrict__ keys,
                                                        Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -182,8 +181,8 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
     const int2 r = rc.rec[c];
     const int v = r.x;
     const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
-    const int stop = min(r.y + kBinChunk, end);
-    const unsigned hv = gc_h(vhash, v);
+    const int stop = min(r.y + chunk, end);
+    const unsigned long long kv = __ldg(&keys[n - 1 - v]);
     for (int i0 = r.y; i0 < stop; i0 += 32 * kInitBatch) {
       int u[kInitBatch], cls[kInitBatch];
       bool valid[kInitBatch];
@@ -192,7 +191,7 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
         valid[k] = i0 + 32 * k + lane < stop;
         u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
       }
-      gc_class_batch(u, valid, v, end - beg, hv, n, nindex, vhash, status, cls);
+      gc_class_batch(u, valid, v, kv, n, keys, status, cls);
       unsigned bh[kInitBatch];
       int total = 0;
 #pragma unroll
@@ -651,7 +650,7 @@ void gc_layout(Carve& c, int n, int m, GCBufs* b) {
   b->vals1 = c.take<int>((size_t)n);
   b->sort_temp = c.take<unsigned>(radix_temp_words((size_t)n));
   b->vhash = c.take<unsigned>((size_t)n);
-  b->chunks = c.take<int2>(row_chunk_capacity(m));
+  b->chunks = c.take<int2>(row_chunk_capacity(m, kMinChunk));
 }
 
 }  // namespace
@@ -677,7 +676,8 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
-  const RowChunks rc{b.chunks, &b.ctl->nchunks, (int)row_chunk_capacity(g.m)};
+  const RowChunks rc{b.chunks, &b.ctl->nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
+  const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
   // key bits that vary: 32 hash bits + enough bits for any degree <= m
   int degbits = 1;
   while (degbits < 31 && ((long long)1 << degbits) <= (long long)g.m) degbits++;
@@ -689,10 +689,12 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
     ECL_LAUNCH(gc_union_hash, grid, kTPB, 0, stream, g.n, uni->vbase, uni->ngraphs, b.vhash);
     vhash = b.vhash;
   }
-  ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, vhash, status);
-  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, vhash, status);
-  mark();
+  // the priority keys first: gc_init compares neighbours by them
   ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
+  ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, b.keys0, status);
+  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, b.keys0,
+             status);
+  mark();
   const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);
   const int* order = in1 ? b.vals1 : b.vals0;
   mark();

@@ -32,7 +32,7 @@ namespace {
 using namespace dev;
 
 constexpr int kTPB = 256;
-constexpr int kLaneMax = 32;
+constexpr int kLaneMax = 32;  // default: lists of up to 32 entries per lane (a launch knob)
 constexpr int kBatch = 4;  // list entries per lane whose loads are issued together
 constexpr unsigned kIn = 0xfe;
 
@@ -140,7 +140,7 @@ __device__ __forceinline__ void mis_clear_list(unsigned* st4, const int* nlist, 
 
 __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, unsigned* __restrict__ st4,
-                                                Status* __restrict__ status, int max_sweeps) {
+                                                Status* __restrict__ status, int max_sweeps, int lane_max) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
         end = __ldg(&nindex[v + 1]);
         if (beg < 0 || end < beg || end > m) beg = end = 0;  // reported by mis_init
       }
-      const bool big = und && (end - beg) > kLaneMax;
+      const bool big = und && (end - beg) > lane_max;
       int verdict = kWait;
       if (und && !big) {
         verdict = kJoin;
@@ -302,7 +302,8 @@ ecl_status mis_enqueue(const GraphDev& g, unsigned char* out, char* ws, Status* 
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mis_run, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   ECL_CUDA_TRY(launch_cooperative(mis_run, dev.sms * std::min(occ, dev.max_threads_per_sm / kTPB), kTPB, stream, g.n,
-                                  g.m, g.nindex, g.nlist, st4, status, max_sweeps));
+                                  g.m, g.nindex, g.nlist, st4, status, max_sweeps,
+                                  bins_of(dev, Bins{kLaneMax, kBinChunk}).lane));
   mark();
   ECL_LAUNCH(mis_emit, grid, kTPB, 0, stream, g.n, st4, out);
   mark();

@@ -15,7 +15,7 @@
 //    Boruvka pass then runs on ~1.6 M instead of ~6.4 M edges, and the
 //    flattened heavy pass absorbs the rest (factor 3 -> 0.75: MST 6.5 -> 5.0 ms);
 //  * mst_scan: builds a worklist of int4 {a, b, weight, j} from the CSR,
-//    lane-level for lists <= 32 entries, warp-level up to kChunk, chunk
+//    lane-level for lists <= 32 entries, warp-level up to 256, chunk
 //    records beyond; appends are staged per warp in shared memory and
 //    reserved in the global list with one atomic per ~kStage entries;
 //    the heavy pass drops entries whose endpoints are already joined (the
@@ -43,8 +43,9 @@ using namespace dev;
 typedef unsigned long long u64;
 
 constexpr int kTPB = 256;
-constexpr int kLaneMax = 32;
-constexpr int kChunk = 256;  // R-MAT's heavy low-id rows share warp groups: keep warp-level rows short
+// Default degree bins: rows of <= 32 entries per lane, chunk records of 256
+// entries (R-MAT's heavy low-id rows share warp groups: keep warp rows short).
+constexpr Bins kMstBins{32, 256};
 constexpr int kMaxRounds = 64;
 constexpr int kSamples = 1024;
 
@@ -234,7 +235,7 @@ template <bool kLight>
 __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __restrict__ nindex,
                                                  const int* __restrict__ nlist, const int* __restrict__ eweight,
                                                  int* __restrict__ parent, int4* __restrict__ wl, int cap,
-                                                 MSTCtl* __restrict__ ctl, int2* __restrict__ chunks,
+                                                 MSTCtl* __restrict__ ctl, int2* __restrict__ chunks, Bins bins,
                                                  Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -256,19 +257,19 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
       }
     }
     const int deg = end - beg;
-    const bool lanelvl = deg > 0 && deg <= kLaneMax;
+    const bool lanelvl = deg > 0 && deg <= bins.lane;
     int rv = v;
     if (!kLight && deg > 0 && v < n) rv = ld(&parent[v]);
     if (kLight)  // chunk records are built once, in the light pass
-      push_chunks_warp<kChunk>(RowChunks{chunks, &ctl->nchunks, (int)row_chunk_capacity(m, kChunk)}, deg > kChunk, v,
-                               beg, end, status);
+      push_chunks_warp(RowChunks{chunks, &ctl->nchunks, (int)row_chunk_capacity(m, kMinChunk)}, bins.chunk,
+                       deg > bins.chunk, v, beg, end, status);
     // lane level: all lanes step through offset k together
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch)
       mst_emit_batch<kLight>(beg + k0, 1, end, lanelvl, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
                              overflow, status);
     // warp level
-    unsigned todo = __ballot_sync(kFull, deg > kLaneMax && deg <= kChunk);
+    unsigned todo = __ballot_sync(kFull, deg > bins.lane && deg <= bins.chunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
@@ -291,7 +292,7 @@ template <bool kLight>
 __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict__ nindex, const int* __restrict__ nlist,
                                                    const int* __restrict__ eweight, int* __restrict__ parent,
                                                    int4* __restrict__ wl, int cap, MSTCtl* __restrict__ ctl,
-                                                   const int2* __restrict__ chunks, int chunk_cap,
+                                                   const int2* __restrict__ chunks, int chunk_cap, int chunk,
                                                    Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
   for (int c = warp; c < total; c += nwarps) {
     const int2 rec = chunks[c];
     const int v = rec.x;
-    const int end = min(rec.y + kChunk, __ldg(&nindex[v + 1]));
+    const int end = min(rec.y + chunk, __ldg(&nindex[v + 1]));
     const int rv = kLight ? v : ld(&parent[v]);
     for (int i0 = rec.y; i0 < end; i0 += 32 * kScanBatch)
       mst_emit_batch<kLight>(i0 + lane, 32, end, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
@@ -473,8 +474,8 @@ void mst_layout(Carve& c, int n, int m, bool symmetric, MSTBufs* b) {
   b->ctl = c.take<MSTCtl>(1);
   b->parent = c.take<int>((size_t)n);
   b->minv = c.take<u64>((size_t)2 * n);
-  b->chunks = c.take<int2>(row_chunk_capacity(m, kChunk));
-  b->chunk_cap = (int)row_chunk_capacity(m, kChunk);
+  b->chunks = c.take<int2>(row_chunk_capacity(m, kMinChunk));
+  b->chunk_cap = (int)row_chunk_capacity(m, kMinChunk);
   // v<n entries: at most m/2 in a symmetric, self-loop-free graph, else m.
   b->cap = symmetric ? m / 2 + 1 : (m > 0 ? m : 1);
   b->wlA = c.take<int4>((size_t)b->cap);
@@ -501,6 +502,7 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
+  const Bins bins = bins_of(dev, kMstBins);
   if (total_dev) *total_dev = &b.ctl->total;
   ECL_CUDA_TRY(cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), stream));
   if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));
@@ -512,15 +514,15 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
     for (int pass = 0; pass < 2; pass++) {
       if (pass == 0) {
         ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, status);
+                   b.cap, b.ctl, b.chunks, bins, status);
         ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, b.chunk_cap, status);
+                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, status);
       } else {
         ECL_LAUNCH(mst_flatten, grid, kTPB, 0, stream, g.n, b.parent);
         ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, status);
+                   b.cap, b.ctl, b.chunks, bins, status);
         ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, b.chunk_cap, status);
+                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, status);
       }
       mark();
       ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.cap, b.parent,

@@ -11,9 +11,19 @@ constexpr int kWarpSlice = kRadixTile / kWarps;  // 512 consecutive keys per war
 
 __device__ __forceinline__ unsigned digit_of(unsigned long long k, int shift) { return (unsigned)(k >> shift) & 0xffu; }
 
+// Element count of this sort: n_max, or the device-side count when one is
+// given (clamped to n_max, the size the launches were made for).
+__device__ __forceinline__ int sort_count(int n_max, const int* n_dev) {
+  if (!n_dev) return n_max;
+  const int c = *n_dev;
+  return c < 0 ? 0 : (c > n_max ? n_max : c);
+}
+
 // counts[d * tiles + t] = number of keys of tile t with digit d.
-__global__ void __launch_bounds__(kThreads) rs_histogram(const unsigned long long* __restrict__ keys, int n, int shift,
+__global__ void __launch_bounds__(kThreads) rs_histogram(const unsigned long long* __restrict__ keys, int n_max,
+                                                         const int* __restrict__ n_dev, int shift,
                                                          unsigned* __restrict__ counts, int tiles) {
+  const int n = sort_count(n_max, n_dev);
   __shared__ unsigned h[256];
   h[threadIdx.x] = 0;
   __syncthreads();
@@ -71,12 +81,14 @@ __global__ void __launch_bounds__(256) rs_scan_digits(unsigned* __restrict__ row
 
 __global__ void __launch_bounds__(kThreads) rs_scatter(const unsigned long long* __restrict__ kin,
                                                        const int* __restrict__ vin, unsigned long long* __restrict__ kout,
-                                                       int* __restrict__ vout, int n, int shift,
-                                                       const unsigned* __restrict__ offsets,
+                                                       int* __restrict__ vout, int n_max, const int* __restrict__ n_dev,
+                                                       int shift, const unsigned* __restrict__ offsets,
                                                        const unsigned* __restrict__ digitbase, int tiles) {
   __shared__ unsigned wcount[kWarps][256];  // per-warp digit counts, then per-warp bases
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = blockIdx.x;
+  const int n = sort_count(n_max, n_dev);
+  if (t * kRadixTile >= n) return;  // a tile past the device-side count: nothing to place
   const int wbase = t * kRadixTile + warp * kWarpSlice;
   for (int d = lane; d < 256; d += 32) wcount[warp][d] = 0;
   __syncwarp();
@@ -127,7 +139,7 @@ __global__ void __launch_bounds__(kThreads) rs_scatter(const unsigned long long*
 }  // namespace
 
 bool radix_sort_pairs(unsigned long long* k0, int* v0, unsigned long long* k1, int* v1, int n, int begin_bit,
-                      int end_bit, unsigned* temp, cudaStream_t stream) {
+                      int end_bit, unsigned* temp, cudaStream_t stream, const int* n_dev) {
   const int tiles = (int)radix_tiles((size_t)n);
   bool flip = false;
   for (int shift = begin_bit; shift < end_bit; shift += 8) {
@@ -136,10 +148,10 @@ bool radix_sort_pairs(unsigned long long* k0, int* v0, unsigned long long* k1, i
     unsigned long long* ko = flip ? k0 : k1;
     int* vo = flip ? v0 : v1;
     unsigned* digitbase = temp + (size_t)256 * tiles;
-    ECL_LAUNCH(rs_histogram, tiles, kThreads, 0, stream, ki, n, shift, temp, tiles);
+    ECL_LAUNCH(rs_histogram, tiles, kThreads, 0, stream, ki, n, n_dev, shift, temp, tiles);
     ECL_LAUNCH(rs_scan_rows, 256, 1024, 0, stream, temp, tiles, digitbase);
     ECL_LAUNCH(rs_scan_digits, 1, 256, 0, stream, digitbase);
-    ECL_LAUNCH(rs_scatter, tiles, kThreads, 0, stream, ki, vi, ko, vo, n, shift, temp, digitbase, tiles);
+    ECL_LAUNCH(rs_scatter, tiles, kThreads, 0, stream, ki, vi, ko, vo, n, n_dev, shift, temp, digitbase, tiles);
     flip = !flip;
   }
   return flip;

@@ -29,8 +29,11 @@ inline size_t radix_temp_words(size_t n) { return 256 * radix_tiles(n) + 256; }
 
 // Sorts keys[0..n) ascending by bits [begin_bit, end_bit) together with vals.
 // Ping-pongs between (k0, v0) and (k1, v1); returns true when the result is
-// in (k1, v1).  Launches are counted and stream-ordered on `stream`.
+// in (k1, v1).  Launches are counted and stream-ordered on `stream`.  With
+// n_dev, the element count is read on the device when the sort runs (at most
+// n, which sizes the launches and the temp buffer), so a count produced by an
+// earlier kernel needs no host round trip.
 bool radix_sort_pairs(unsigned long long* k0, int* v0, unsigned long long* k1, int* v1, int n, int begin_bit,
-                      int end_bit, unsigned* temp, cudaStream_t stream);
+                      int end_bit, unsigned* temp, cudaStream_t stream, const int* n_dev = nullptr);
 
 }  // namespace ecl

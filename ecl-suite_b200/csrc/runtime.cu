@@ -18,14 +18,18 @@ ecl_tune g_tune{};  // process-wide knobs of the single-graph entry points (unde
 }  // namespace
 
 bool tune_valid(const ecl_tune& t) {
+  const bool chunk_ok = t.row_chunk == 0 || (t.row_chunk >= dev::kMinChunk && t.row_chunk <= dev::kMaxChunk &&
+                                              (t.row_chunk & (t.row_chunk - 1)) == 0);
   return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 8 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
-         t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864;
+         t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok;
 }
 
 void apply_tune(DeviceInfo* d, const ecl_tune& t) {
   d->blocks_per_sm = t.blocks_per_sm;
   d->mst_light_factor = t.mst_light_factor;
   d->gc_core_ranks = t.gc_core_ranks;
+  d->row_lane_max = t.row_lane_max;
+  d->row_chunk = t.row_chunk;
 }
 
 void set_last_error(const char* where, cudaError_t e) {

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "csr_bins.cuh"
 #include "ecl_b200.h"
 
 namespace ecl {
@@ -69,6 +70,8 @@ struct DeviceInfo {
   int blocks_per_sm = 0;
   float mst_light_factor = 0.f;
   int gc_core_ranks = 0;  // GC: ranks coloured in one CTA's shared memory (0 = default)
+  int row_lane_max = 0;   // degree bins of the CSR scans (0 = each scan's default)
+  int row_chunk = 0;
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }
@@ -79,6 +82,11 @@ ecl_status current_device(DeviceInfo* info);
 // Range check of a knob set, and its application to a DeviceInfo.
 bool tune_valid(const ecl_tune& t);
 void apply_tune(DeviceInfo* d, const ecl_tune& t);
+
+// Degree bins of a scan: the knobs of `d` where set, else the scan's default.
+inline dev::Bins bins_of(const DeviceInfo& d, dev::Bins dflt) {
+  return dev::Bins{d.row_lane_max > 0 ? d.row_lane_max : dflt.lane, d.row_chunk > 0 ? d.row_chunk : dflt.chunk};
+}
 
 // Workspace carving: the same sequence of take() calls sizes a workspace
 // (base == nullptr) and then hands out 256-byte-aligned sub-buffers.

@@ -77,7 +77,7 @@ __device__ __forceinline__ bool io_raise(unsigned long long* p, unsigned long lo
 // out-entry other than self-loops.  Both facts share one flag word per vertex
 // (kHasIn | kHasOut), so the liveness test is one load; scc_mark ORs kHasIn
 // into flags[w] for every entry w != v and kHasOut into flags[v] for every v
-// with such an entry; rows longer than kBinChunk go to chunk records.
+// with such an entry; rows longer than bins.chunk go to chunk records.
 constexpr int kHasIn = 1, kHasOut = 2;
 
 // Marks kScanBatch entries w[k] (present where valid[k]) of v's list, at CSR
@@ -109,7 +109,8 @@ __device__ __forceinline__ void scc_mark_batch(const bool (&valid)[kScanBatch], 
 
 __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __restrict__ nindex,
                                                  const int* __restrict__ nlist, int* __restrict__ flags,
-                                                 int2* __restrict__ wl, RowChunks rc, Status* __restrict__ status) {
+                                                 int2* __restrict__ wl, RowChunks rc, Bins bins,
+                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -118,9 +119,9 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
     int beg = 0, end = 0;
     if (v < n) csr_row(nindex, v, m, beg, end, status);
     const int deg = end - beg;
-    push_chunks_warp<kBinChunk>(rc, deg > kBinChunk, v, beg, end, status);
+    push_chunks_warp(rc, bins.chunk, deg > bins.chunk, v, beg, end, status);
     bool out = false;
-    const bool lanelvl = deg <= kBinLane;
+    const bool lanelvl = deg <= bins.lane;
     const int kmax = __reduce_max_sync(kFull, lanelvl ? deg : 0);
     for (int k0 = 0; k0 < kmax; k0 += kScanBatch) {
       int w[kScanBatch], j[kScanBatch];
@@ -133,7 +134,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       }
       scc_mark_batch(valid, v, w, j, n, flags, wl, out, status);
     }
-    unsigned todo = __ballot_sync(kFull, deg > kBinLane && deg <= kBinChunk);
+    unsigned todo = __ballot_sync(kFull, deg > bins.lane && deg <= bins.chunk);
     while (todo) {
       const int who = __ffs(todo) - 1;
       todo &= todo - 1;
@@ -154,13 +155,13 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       }
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
-    if (v < n && deg <= kBinChunk && out) fetch_or(&flags[v], kHasOut);  // long rows: scc_mark_chunks
+    if (v < n && deg <= bins.chunk && out) fetch_or(&flags[v], kHasOut);  // long rows: scc_mark_chunks
   }
 }
 
 __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
                                                         const int* __restrict__ nlist, int* __restrict__ flags,
-                                                        int2* __restrict__ wl, RowChunks rc,
+                                                        int2* __restrict__ wl, RowChunks rc, int chunk,
                                                         Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -168,7 +169,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
   const int total = chunk_total(rc);
   for (int c = warp; c < total; c += nwarps) {
     const int2 r = rc.rec[c];
-    const int end = min(r.y + kBinChunk, __ldg(&nindex[r.x + 1]));
+    const int end = min(r.y + chunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
     for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) {
       int w[kScanBatch], j[kScanBatch];
@@ -345,7 +346,7 @@ void scc_layout(Carve& c, int n, int m, SCCBufs* b) {
   b->rounds = c.take<SCCRound>((size_t)b->max_rounds);
   b->flags = c.take<int>((size_t)n);
   b->nchunks = c.take<int>(64);
-  b->chunks = c.take<int2>(row_chunk_capacity(m));
+  b->chunks = c.take<int2>(row_chunk_capacity(m, kMinChunk));
   b->io = c.take<unsigned long long>((size_t)n);
   b->wlA = c.take<int2>((size_t)(m > 0 ? m : 1));
   b->wlB = c.take<int2>((size_t)(m > 0 ? m : 1));
@@ -381,9 +382,10 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
     return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.flags, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
-  const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m)};
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, status);
+  const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
+  const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins, status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, status);
   mark();
   ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label,
                                   b.ctl, b.rounds, max_rounds, status));

@@ -384,7 +384,8 @@ BATCH_CC, BATCH_MIS, BATCH_GC, BATCH_MST, BATCH_SCC = 0x1, 0x2, 0x4, 0x8, 0x10
 class Tune(C.Structure):
     """ecl_tune: launch knobs (0 = built-in default); they never change results."""
 
-    _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float), ("gc_core_ranks", C.c_int32)]
+    _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float), ("gc_core_ranks", C.c_int32),
+                ("row_lane_max", C.c_int32), ("row_chunk", C.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -421,13 +422,15 @@ _sig("ecl_batch_build", C.c_int, [_PB, C.c_uint32, C.c_int64, _VP])
 _sig("ecl_batch_run", C.c_int, [_PB, _PO])
 _sig("ecl_batch_tune", C.c_int, [_PB, _I32, C.POINTER(Tune)])
 _sig("ecl_batch_set_tune", C.c_int, [_PB, C.POINTER(Tune)])
+_sig("ecl_batch_tune_points", C.c_int32, [_PB])
 _sig("ecl_batch_graphs", C.c_int32, [_PB])
 _sig("ecl_batch_superbatches", C.c_int32, [_PB])
 _sig("ecl_batch_graph_size", C.c_int, [_PB, _I32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)])
 _sig("ecl_batch_graph_csr", C.c_int, [_PB, _I32, _VP, _VP, _VP])
 _sig("ecl_batch_result", C.c_int, [_PB, _I32, C.c_uint32, _VP, C.POINTER(C.c_uint64)])
 EXPORTED += ["ecl_batch_create", "ecl_batch_destroy", "ecl_batch_add", "ecl_batch_add_mix", "ecl_batch_build",
-             "ecl_batch_run", "ecl_batch_tune", "ecl_batch_set_tune", "ecl_batch_graphs", "ecl_batch_superbatches",
+             "ecl_batch_run", "ecl_batch_tune", "ecl_batch_set_tune", "ecl_batch_tune_points", "ecl_batch_graphs",
+             "ecl_batch_superbatches",
              "ecl_batch_graph_size", "ecl_batch_graph_csr", "ecl_batch_result"]
 
 
@@ -467,6 +470,11 @@ class Batch:
         t = Tune()
         _check(lib.ecl_batch_tune(self.h, trials, C.byref(t)), "ecl_batch_tune")
         return t
+
+    @property
+    def tune_points(self) -> int:
+        """Knob settings the last tune() timed."""
+        return int(lib.ecl_batch_tune_points(self.h))
 
     @property
     def graphs(self) -> int:

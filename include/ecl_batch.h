@@ -59,11 +59,16 @@ ecl_status ecl_batch_build(ecl_batch* b, uint32_t codes, int64_t max_entries, vo
  * opts->elapsed_ms receives the device time of the run. */
 ecl_status ecl_batch_run(ecl_batch* b, ecl_opts* opts);
 
-/* Tries each candidate knob setting on the built batch (`trials` timed runs
- * each), keeps the fastest and returns it in *best (may be NULL).  Rebuilds
- * the captured CUDA graph. */
+/* The autotuner: coordinate descent over the launch knobs of ecl_tune on the
+ * built batch (grid size, the per-lane / chunk row thresholds of the CSR
+ * scans, the MST light-edge split and, with GC, GC's shared-memory core); each
+ * setting costs one capturing run plus `trials` timed runs.  Keeps the
+ * fastest, returns it in *best (may be NULL) and rebuilds the captured CUDA
+ * graph.  Results never depend on the knobs. */
 ecl_status ecl_batch_tune(ecl_batch* b, int32_t trials, ecl_tune* best);
 ecl_status ecl_batch_set_tune(ecl_batch* b, const ecl_tune* t);
+/* Number of knob settings the last ecl_batch_tune timed. */
+int32_t ecl_batch_tune_points(const ecl_batch* b);
 
 int32_t ecl_batch_graphs(const ecl_batch* b);
 int32_t ecl_batch_superbatches(const ecl_batch* b);

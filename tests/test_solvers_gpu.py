@@ -273,3 +273,26 @@ def test_cc_validate_checks_the_symmetric_flag(ecl):
     with pytest.raises(ecl.EclError) as e:
         ecl.cc(g, validate=True)
     assert e.value.status == ecl.ERR_BAD_GRAPH
+
+
+@pytest.mark.parametrize("knobs", [dict(row_lane_max=1, row_chunk=128), dict(row_lane_max=8, row_chunk=512),
+                                   dict(row_lane_max=32, row_chunk=8192, blocks_per_sm=2),
+                                   dict(mst_light_factor=0.4, gc_core_ranks=5)])
+def test_launch_knobs_never_change_results(ecl, orc, knobs):
+    """Every code under non-default degree bins, grid sizes, MST split and GC
+    core size gives the oracle's result (hub rows cross every chunk size)."""
+    old = ecl.set_tune(**knobs)
+    try:
+        g = weighted(ecl.gen_rmat(15, 16, seed=2))
+        hub = undirected(9000, [(8999, i) for i in range(8999)] + [(i, i + 1) for i in range(0, 200, 2)])
+        for h in (g, hub):
+            assert np.array_equal(ecl.cc(h), orc.cc(h)), knobs
+            assert np.array_equal(ecl.mis(h), orc.mis(h)), knobs
+            assert np.array_equal(ecl.gc(h), orc.gc(h)), knobs
+        inm, tot = ecl.mst(g)
+        einm, etot = orc.mst(g)
+        assert tot == etot and np.array_equal(inm, einm), knobs
+        d = ecl.gen_rmat(14, 16, seed=2, symmetrise=False)
+        assert np.array_equal(ecl.scc(d), orc.scc(d)), knobs
+    finally:
+        ecl.set_tune(old)
