@@ -62,7 +62,7 @@ __global__ void batch_mst_totals(int ngraphs, const int* __restrict__ ebase, con
   for (int g = warp; g < ngraphs; g += nwarps) {
     unsigned long long s = 0;
     for (int j = __ldg(&ebase[g]) + lane; j < __ldg(&ebase[g + 1]); j += 32)
-      if (in_mst[j]) s += (unsigned)__ldg(&eweight[j]);
+      if (in_mst[j]) s += (unsigned)__ldg(&eweight[j]);  // race-free: in_mst is final (MST finished)
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFull, s, o);
     if (lane == 0) totals[g] = s;
   }

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(kTPB) cc_init(int n, int m, const int* __restr
         break;
       }
     }
-    parent[v] = p;
+    parent[v] = p;  // race-free: thread-owned init, no reader in this launch
   }
 }
 
@@ -336,7 +336,7 @@ __global__ void __launch_bounds__(kTPB) cc_mark_giant(int n, const int* __restri
                                                       const CCCounters* __restrict__ ctr,
                                                       unsigned char* __restrict__ ing) {
   const int gr = ctr->giant;
-  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) ing[v] = parent[v] == gr;
+  for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) ing[v] = parent[v] == gr;  // race-free: parent is not written in this launch
 }
 
 // Remaining entries of vertices outside the giant component.  An entry is

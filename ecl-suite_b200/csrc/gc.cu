@@ -164,7 +164,8 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       }
       if (lane == who) h = wh;
     }
-    if (v < n) hc[v] = dv > bins.chunk ? 0 : h;  // chunked rows start at 0, counted by gc_init_chunks
+    // race-free: v's own count, read only by later launches; chunked rows start at 0 (gc_init_chunks adds)
+    if (v < n) hc[v] = dv > bins.chunk ? 0 : h;
   }
 }
 

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kTPB) mis_init(int n, int m, const int* __rest
       }
       word |= b << (8 * k);
     }
-    st4[w] = word;
+    st4[w] = word;  // race-free: thread-owned init, no reader in this launch
   }
 }
 
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kTPB) mis_run(int n, int m, const int* __restr
 __global__ void __launch_bounds__(kTPB) mis_emit(int n, const unsigned* __restrict__ st4,
                                                  unsigned char* __restrict__ out) {
   for (int v = blockIdx.x * kTPB + threadIdx.x; v < n; v += gridDim.x * kTPB) {
-    out[v] = (unsigned char)byte_of(st4[v >> 2], v);
+    out[v] = (unsigned char)byte_of(st4[v >> 2], v);  // race-free: st4 is final (mis_run finished)
   }
 }
 

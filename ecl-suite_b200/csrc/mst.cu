@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(kTPB) mst_flatten(int n, int* __restrict__ par
 
 __global__ void mst_init(int n, int* __restrict__ parent, u64* __restrict__ minv) {
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    // race-free: thread-owned init, no reader in this launch
     parent[v] = v;
     minv[v] = ~0ull;
     minv[n + v] = ~0ull;
@@ -445,7 +446,7 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
       const u64 key = ((u64)(unsigned)e.z << 32) | (unsigned)e.w;
       if (valid && (key == kx || key == ky)) {
         mst_join(e.x, e.y, parent);
-        in_mst[e.w] = 1;  // each entry j is joined at most once: plain byte store
+        in_mst[e.w] = 1;  // race-free: each entry j is joined at most once, and never read here
         local += (u64)(unsigned)e.z;
       }
     }

@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(kTPB, 4) scc_solve(int n, int m0, int2* __rest
   const int nthreads = gridDim.x * kTPB;
   // 0. live vertices start at (v, v); trimmed ones are DEAD
   for (int v = tid; v < n; v += nthreads)
-    io[v] = __ldg(&flags[v]) == (kHasIn | kHasOut) ? io_pack(v, v) : kDead;
+    io[v] = __ldg(&flags[v]) == (kHasIn | kHasOut) ? io_pack(v, v) : kDead;  // race-free: owned, barrier next
   if (!grid_sync(&ctl->bar, status)) return;
   int size = m0;
   int sweep = 0;
@@ -309,9 +309,9 @@ __global__ void __launch_bounds__(kTPB, 4) scc_solve(int n, int m0, int2* __rest
     for (int v = tid; v < n; v += nthreads) {
       const unsigned long long A = ld(&io[v]);
       if (A == kDead) {
-        label[v] = v;
+        label[v] = v;  // race-free: the output, thread-owned and never read here
       } else if (io_in(A) == io_out(A)) {
-        label[v] = io_in(A);
+        label[v] = io_in(A);  // race-free: as above
       } else {
         st(&io[v], io_pack(v, v));
         again = true;
