@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kTPB) gc_union_hash(int n, const int* __restri
 
 __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restrict__ nindex,
                                                 const int* __restrict__ nlist, int* __restrict__ nl2,
-                                                int* __restrict__ hc, RowChunks rc, Bins bins,
+                                                int* __restrict__ hc, RowChunks rc, Bins bins, bool vec,
                                                 const unsigned long long* __restrict__ keys,
                                                 Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
@@ -146,14 +146,8 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       const int wend = __shfl_sync(kFull, end, who);
       const unsigned long long wkv = __shfl_sync(kFull, kv, who);
       int wh = 0;
-      for (int i0 = wbeg; i0 < wend; i0 += 32 * kInitBatch) {
-        int u[kInitBatch], cls[kInitBatch];
-        bool valid[kInitBatch];
-#pragma unroll
-        for (int k = 0; k < kInitBatch; k++) {
-          valid[k] = i0 + 32 * k + lane < wend;
-          u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
-        }
+      warp_row(wbeg, wend, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
+        int cls[kInitBatch];
         gc_class_batch(u, valid, wv, wkv, n, keys, status, cls);
 #pragma unroll
         for (int k = 0; k < kInitBatch; k++) {
@@ -161,7 +155,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
           if (cls[k] == 1) nl2[wbeg + wh + __popc(bh & ((1u << lane) - 1))] = u[k];
           wh += __popc(bh);
         }
-      }
+      });
       if (lane == who) h = wh;
     }
     // race-free: v's own count, read only by later launches; chunked rows start at 0 (gc_init_chunks adds)
@@ -171,7 +165,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
 
 __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ nl2,
-                                                       int* __restrict__ hc, RowChunks rc, int chunk,
+                                                       int* __restrict__ hc, RowChunks rc, int chunk, bool vec,
                                                        const unsigned long long* __restrict__ keys,
                                                        Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
@@ -184,31 +178,25 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
     const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
     const int stop = min(r.y + chunk, end);
     const unsigned long long kv = __ldg(&keys[n - 1 - v]);
-    for (int i0 = r.y; i0 < stop; i0 += 32 * kInitBatch) {
-      int u[kInitBatch], cls[kInitBatch];
-      bool valid[kInitBatch];
-#pragma unroll
-      for (int k = 0; k < kInitBatch; k++) {
-        valid[k] = i0 + 32 * k + lane < stop;
-        u[k] = valid[k] ? __ldg(&nlist[i0 + 32 * k + lane]) : 0;
-      }
+    warp_row(r.y, stop, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
+      int cls[kInitBatch];
       gc_class_batch(u, valid, v, kv, n, keys, status, cls);
       unsigned bh[kInitBatch];
-      int total = 0;
+      int nh = 0;
 #pragma unroll
       for (int k = 0; k < kInitBatch; k++) {
         bh[k] = __ballot_sync(kFull, cls[k] == 1);
-        total += __popc(bh[k]);
+        nh += __popc(bh[k]);
       }
       int hbase = 0;
-      if (lane == 0 && total) hbase = fetch_add(&hc[v], total);
+      if (lane == 0 && nh) hbase = fetch_add(&hc[v], nh);
       hbase = __shfl_sync(kFull, hbase, 0);
 #pragma unroll
       for (int k = 0; k < kInitBatch; k++) {
         if (cls[k] == 1) nl2[beg + hbase + __popc(bh[k] & ((1u << lane) - 1))] = u[k];
         hbase += __popc(bh[k]);
       }
-    }
+    });
   }
 }
 
@@ -692,8 +680,9 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   }
   // the priority keys first: gc_init compares neighbours by them
   ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
-  ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, b.keys0, status);
-  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, b.keys0,
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0;  // 16-byte row loads
+  ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, vec, b.keys0, status);
+  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, vec, b.keys0,
              status);
   mark();
   const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);

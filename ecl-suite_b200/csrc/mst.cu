@@ -226,6 +226,77 @@ __device__ __forceinline__ void mst_emit_batch(int j0, int stride, int jend, boo
   }
 }
 
+// Emits the worklist entries of one warp-walked row segment [jb, je) of v:
+// the unaligned head (up to 3 entries) and tail go through mst_emit_batch;
+// the 16-byte-aligned middle is read with one 16-byte load of nlist and one
+// of eweight per lane (4 consecutive entries a lane), so a warp step covers
+// 128 entries with two load instructions instead of eight.  vec = false
+// (nlist or eweight not 16-byte aligned) keeps the scalar loads throughout.
+// All lanes call.
+template <bool kLight>
+__device__ __forceinline__ void mst_emit_row(int jb, int je, bool vec, int v, int rv, int n, const int* nlist,
+                                             const int* eweight, int thr, const int* parent, Stage& stg, int4* wl,
+                                             int* cnt, int cap, bool& overflow, Status* status) {
+  const int lane = threadIdx.x & 31;
+  if (!vec) {
+    for (int i0 = jb; i0 < je; i0 += 32 * kScanBatch)
+      mst_emit_batch<kLight>(i0 + lane, 32, je, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                             overflow, status);
+    return;
+  }
+  const int a = min(je, (jb + 3) & ~3);  // first 16-byte boundary
+  const int z = max(a, je & ~3);         // last one
+  if (jb < a)
+    mst_emit_batch<kLight>(jb + lane, 32, a, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                           overflow, status);
+  for (int i0 = a; i0 < z; i0 += 4 * 32) {
+    const int j0 = i0 + 4 * lane;
+    const bool active = j0 < z;  // z - a is a multiple of 4: a lane's 4 entries are all in or all out
+    int u[4] = {-1, -1, -1, -1}, w[4] = {0, 0, 0, 0}, ru[4];
+    if (active) {
+      const int4 x = __ldg(reinterpret_cast<const int4*>(nlist + j0));
+      u[0] = x.x, u[1] = x.y, u[2] = x.z, u[3] = x.w;
+      if (x.x > v || x.y > v || x.z > v || x.w > v) {
+        const int4 y = __ldg(reinterpret_cast<const int4*>(eweight + j0));
+        w[0] = y.x, w[1] = y.y, w[2] = y.z, w[3] = y.w;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      ru[k] = (!kLight && (unsigned)u[k] < (unsigned)n && u[k] > v && mst_keep<false>(w[k], thr))
+                  ? ld(&parent[u[k]])  // flat after mst_flatten
+                  : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int j = j0 + k;
+      bool keep = false;
+      int4 e = make_int4(0, 0, 0, 0);
+      if (active) {
+        if ((unsigned)u[k] >= (unsigned)n) {
+          raise(status, ECL_ERR_BAD_GRAPH, u[k]);
+        } else if (u[k] > v) {
+          if (w[k] < 0) {
+            raise(status, ECL_ERR_BAD_GRAPH, j);
+          } else if (mst_keep<kLight>(w[k], thr)) {
+            if (kLight) {
+              keep = true;
+              e = make_int4(v, u[k], w[k], j);
+            } else {
+              keep = ru[k] != rv;
+              e = make_int4(rv, ru[k], w[k], j);
+            }
+          }
+        }
+      }
+      stg.push(keep, e, wl, cnt, cap, overflow);
+    }
+  }
+  if (z < je)
+    mst_emit_batch<kLight>(z + lane, 32, je, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
+                           overflow, status);
+}
+
 // More v<n entries than the worklist holds: an asymmetric graph flagged
 // symmetric.
 __device__ __forceinline__ void mst_overflow(bool overflow, Status* status) {
@@ -237,7 +308,7 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
                                                  const int* __restrict__ nlist, const int* __restrict__ eweight,
                                                  int* __restrict__ parent, int4* __restrict__ wl, int cap,
                                                  MSTCtl* __restrict__ ctl, int2* __restrict__ chunks, Bins bins,
-                                                 Status* __restrict__ status) {
+                                                 bool vec, Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
@@ -278,9 +349,8 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
       const int wrv = __shfl_sync(kFull, rv, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      for (int i0 = wbeg; i0 < wend; i0 += 32 * kScanBatch)
-        mst_emit_batch<kLight>(i0 + lane, 32, wend, true, wv, wrv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
-                               overflow, status);
+      mst_emit_row<kLight>(wbeg, wend, vec, wv, wrv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow,
+                           status);
     }
   }
   stg.flush(wl, cnt, cap, overflow);
@@ -294,8 +364,7 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
                                                    const int* __restrict__ eweight, int* __restrict__ parent,
                                                    int4* __restrict__ wl, int cap, MSTCtl* __restrict__ ctl,
                                                    const int2* __restrict__ chunks, int chunk_cap, int chunk,
-                                                   Status* __restrict__ status) {
-  const int lane = threadIdx.x & 31;
+                                                   bool vec, Status* __restrict__ status) {
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   const int thr = ctl->threshold;
@@ -309,9 +378,7 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
     const int v = rec.x;
     const int end = min(rec.y + chunk, __ldg(&nindex[v + 1]));
     const int rv = kLight ? v : ld(&parent[v]);
-    for (int i0 = rec.y; i0 < end; i0 += 32 * kScanBatch)
-      mst_emit_batch<kLight>(i0 + lane, 32, end, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
-                             overflow, status);
+    mst_emit_row<kLight>(rec.y, end, vec, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow, status);
   }
   stg.flush(wl, cnt, cap, overflow);
   mst_overflow(overflow, status);
@@ -504,6 +571,8 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
   const Bins bins = bins_of(dev, kMstBins);
+  // 16-byte row loads need 16-byte-aligned arrays (entries j = 0 mod 4 then are)
+  const bool vec = ((reinterpret_cast<uintptr_t>(g.nlist) | reinterpret_cast<uintptr_t>(g.eweight)) & 15) == 0;
   if (total_dev) *total_dev = &b.ctl->total;
   ECL_CUDA_TRY(cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), stream));
   if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));
@@ -515,15 +584,15 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
     for (int pass = 0; pass < 2; pass++) {
       if (pass == 0) {
         ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, bins, status);
+                   b.cap, b.ctl, b.chunks, bins, vec, status);
         ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, status);
+                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, vec, status);
       } else {
         ECL_LAUNCH(mst_flatten, grid, kTPB, 0, stream, g.n, b.parent);
         ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
-                   b.cap, b.ctl, b.chunks, bins, status);
+                   b.cap, b.ctl, b.chunks, bins, vec, status);
         ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
-                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, status);
+                   b.ctl, b.chunks, b.chunk_cap, bins.chunk, vec, status);
       }
       mark();
       ECL_CUDA_TRY(launch_cooperative(mst_boruvka, coop_grid, kTPB, stream, g.n, pass, b.wlA, b.wlB, b.cap, b.parent,

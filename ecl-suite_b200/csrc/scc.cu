@@ -109,7 +109,7 @@ __device__ __forceinline__ void scc_mark_batch(const bool (&valid)[kScanBatch], 
 
 __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __restrict__ nindex,
                                                  const int* __restrict__ nlist, int* __restrict__ flags,
-                                                 int2* __restrict__ wl, RowChunks rc, Bins bins,
+                                                 int2* __restrict__ wl, RowChunks rc, Bins bins, bool vec,
                                                  Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -142,17 +142,9 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       bool wout = false;
-      for (int i0 = wbeg + lane; i0 < wend; i0 += 32 * kScanBatch) {
-        int w[kScanBatch], j[kScanBatch];
-        bool valid[kScanBatch];
-#pragma unroll
-        for (int k = 0; k < kScanBatch; k++) {
-          j[k] = i0 + 32 * k;
-          valid[k] = j[k] < wend;
-          w[k] = valid[k] ? __ldg(&nlist[j[k]]) : 0;
-        }
+      warp_row(wbeg, wend, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
         scc_mark_batch(valid, wv, w, j, n, flags, wl, wout, status);
-      }
+      });
       if (__any_sync(kFull, wout) && lane == who) out = true;
     }
     if (v < n && deg <= bins.chunk && out) fetch_or(&flags[v], kHasOut);  // long rows: scc_mark_chunks
@@ -161,7 +153,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
 
 __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
                                                         const int* __restrict__ nlist, int* __restrict__ flags,
-                                                        int2* __restrict__ wl, RowChunks rc, int chunk,
+                                                        int2* __restrict__ wl, RowChunks rc, int chunk, bool vec,
                                                         Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
@@ -171,17 +163,9 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     const int2 r = rc.rec[c];
     const int end = min(r.y + chunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
-    for (int i0 = r.y + lane; i0 < end; i0 += 32 * kScanBatch) {
-      int w[kScanBatch], j[kScanBatch];
-      bool valid[kScanBatch];
-#pragma unroll
-      for (int k = 0; k < kScanBatch; k++) {
-        j[k] = i0 + 32 * k;
-        valid[k] = j[k] < end;
-        w[k] = valid[k] ? __ldg(&nlist[j[k]]) : 0;
-      }
+    warp_row(r.y, end, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
       scc_mark_batch(valid, r.x, w, j, n, flags, wl, out, status);
-    }
+    });
     if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
   }
 }
@@ -384,8 +368,10 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
   const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
-  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins, status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, status);
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0;  // 16-byte row loads
+  ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins, vec, status);
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, vec,
+             status);
   mark();
   ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label,
                                   b.ctl, b.rounds, max_rounds, status));
