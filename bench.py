@@ -8,10 +8,22 @@ symmetrised, duplicate- and self-loop-free graph, and SCC on the directed
 graph of the same parameters.  Metric: edges/s = sum of each solve's
 g.edges / sum of solve times, as the reference computes edges/s
 (ECL-CC-atomic.cu:314-316): inputs resident on the device, kernel time only.
-L2 (126 MB) is flushed by a 256 MiB write before every solve.
+L2 (126 MB) is flushed by a 256 MiB write before every solve.  The line also
+carries the end-to-end rate through the C ABI (host CSR in, results out),
+the dominant kernel's roofline, GC's latency roofline (critical path x the
+measured hop cost), a CPU baseline on the same graphs and, on one GPU, the
+other four configs measured after the headline (`other_configs`: the grid
+CC, APSP n=8192, the batched 4096-graph mix, the served Poisson stream),
+each with its own clocks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload suite|grid|apsp] [--scale S]
+                  [--workload suite|grid|apsp|batch|serve] [--scale S]
+                  [--no-other-configs] [--no-cpu-baseline]
+
+--impl reference times the reference's own CPU routines (cpuMST; the C
+restatement where the reference has no CPU solver) on the same graphs, built
+by the restated generators under oracle/ without loading the product, plus
+the reference's race-free CUDA build on them (`reference_gpu`).
 
 Multi-GPU: replicas only -- every rank solves its own copy of the workload, no
 collective on the data path; value = edges of all ranks / max time over ranks.
@@ -603,6 +615,24 @@ def bench_plain(args, rank, world, local_rank):
                 "peak_add_then_min": round(peak_sep, 3),
                 "note": "2 integer ops (add + min) per update of the padded N^3 closure, N = ceil(n/128)*128"}
 
+    # GC's colouring is bound by its dependency chain, not by bytes: the
+    # latency roofline is the longest chain of the input (hops inside the
+    # shared-memory core and after it) times the measured cost of one hop
+    # there, against the measured gc_core + gc_pull time
+    gc_latency = None
+    if args.workload == "suite" and ("gc", 3) in phase_tot:
+        hop = {"l2_backoff": ecl.hop_latency(0), "l2_spin": ecl.hop_latency(1), "smem": ecl.hop_latency(2)}
+        tune = ecl.get_tune()
+        hops, hops_core, path_ns = ecl.gc_critical_path(sym, tune.gc_core_ranks, hop["smem"], hop["l2_backoff"])
+        got_ms = (phase_tot[("gc", 2)] + phase_tot[("gc", 3)]) / args.steps
+        gc_latency = {"kernels": "gc_core+gc_pull", "hops": hops, "hops_in_core": hops_core,
+                      "hop_ns": {k: round(v, 1) for k, v in hop.items()}, "bound_ms": round(path_ns / 1e6, 4),
+                      "achieved_ms": round(got_ms, 4), "frac": round(path_ns / 1e6 / got_ms, 4),
+                      "model": "longest chain of higher-priority dependencies; a hop into the core costs the "
+                               "shared-memory hop, any other the L2 hop with the pull's back-off polling"}
+        if roof is not None and roof.get("kernel") == "gc_pull":
+            roof["latency"] = gc_latency
+
     # end to end through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -681,6 +711,8 @@ def bench_plain(args, rank, world, local_rank):
         "per_code": per_code, "phase_ms": phases, "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": int(launches), "clocks": clocks,
     }
+    if gc_latency is not None:
+        line["gc_latency_roofline"] = gc_latency
     del dgs, ws, outs, flush
     return line
 

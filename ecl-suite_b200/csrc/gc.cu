@@ -36,6 +36,7 @@
 //    chain costs one poll and a short re-check, not a rescan of the row
 //    (short rows: the same with a bit mask per lane).
 #include <algorithm>
+#include <vector>
 
 #include "csr_bins.cuh"
 #include "radix_sort.cuh"
@@ -735,4 +736,67 @@ extern "C" ecl_status ecl_compute_gc(int32_t nodes, int32_t edges, const int32_t
   ecl_graph_view g{nodes, edges, nidx, nlist, nullptr, ECL_HOST, 0};
   ecl_opts o{};
   return ecl_gc(&g, color, &o);
+}
+
+// ---- the colouring's critical path (a host-side diagnostic) --------------------
+//
+// The colour of a vertex is fixed only after every higher-priority neighbour
+// has its own, so no schedule finishes faster than the longest chain of such
+// dependencies.  This walks the priority order once on the host: hops[v] = 1 +
+// the largest hops[u] over v's higher-priority entries u (0 with none), and a
+// time model path[v] = the latest path[u] + the cost of one hop to v -- the
+// shared-memory hop for a vertex the GPU colours in its core (the first
+// min(long rows, core_ranks) ranks), the L2 hop for every other one.  The
+// bench reports the resulting latency bound beside gc_pull's time.
+extern "C" ecl_status ecl_gc_critical_path(const ecl_graph_view* g, int32_t core_ranks, double hop_core_ns,
+                                           double hop_rest_ns, int32_t* hops, int32_t* hops_core, double* path_ns) {
+  using namespace ecl;
+  if (!g || g->location != ECL_HOST || g->nodes < 1 || g->edges < 0 || !g->nindex || (g->edges > 0 && !g->nlist))
+    return ECL_ERR_INVALID_ARG;
+  if (core_ranks < 0 || core_ranks > kCoreMax) return ECL_ERR_INVALID_ARG;
+  const int n = g->nodes;
+  const int* nindex = g->nindex;
+  const int* nlist = g->nlist;
+  for (int v = 0; v < n; v++)
+    if (nindex[v] < 0 || nindex[v + 1] < nindex[v] || nindex[v + 1] > g->edges) return ECL_ERR_BAD_GRAPH;
+  std::vector<unsigned long long> key((size_t)n);
+  int nbig = 0;
+  for (int v = 0; v < n; v++) {
+    const unsigned deg = (unsigned)(nindex[v + 1] - nindex[v]);
+    key[(size_t)v] = ((unsigned long long)deg << 32) | dev::ecl_hash((unsigned)v);
+    nbig += deg > (unsigned)kWarpRow;
+  }
+  std::vector<int> order((size_t)n);
+  for (int v = 0; v < n; v++) order[(size_t)v] = v;
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    return key[(size_t)a] != key[(size_t)b] ? key[(size_t)a] > key[(size_t)b] : a > b;
+  });
+  std::vector<int> rank((size_t)n);
+  for (int r = 0; r < n; r++) rank[(size_t)order[(size_t)r]] = r;
+  const int core = std::min(nbig, core_ranks > 0 ? core_ranks : kCoreDefault);
+  std::vector<int> hop((size_t)n, 0);
+  std::vector<double> path((size_t)n, 0.0);
+  int best = 0, best_core = 0;
+  double best_path = 0.0;
+  for (int r = 0; r < n; r++) {
+    const int v = order[(size_t)r];
+    int h = -1;
+    double t = -1.0;
+    for (int i = nindex[v]; i < nindex[v + 1]; i++) {
+      const int u = nlist[i];
+      if (u < 0 || u >= n) return ECL_ERR_BAD_GRAPH;
+      if (u == v || rank[(size_t)u] > r) continue;
+      h = std::max(h, hop[(size_t)u]);
+      t = std::max(t, path[(size_t)u]);
+    }
+    hop[(size_t)v] = h + 1;
+    path[(size_t)v] = t < 0.0 ? 0.0 : t + (r < core ? hop_core_ns : hop_rest_ns);
+    best = std::max(best, hop[(size_t)v]);
+    if (r < core) best_core = std::max(best_core, hop[(size_t)v]);
+    best_path = std::max(best_path, path[(size_t)v]);
+  }
+  if (hops) *hops = best;
+  if (hops_core) *hops_core = best_core;
+  if (path_ns) *path_ns = best_path;
+  return ECL_OK;
 }

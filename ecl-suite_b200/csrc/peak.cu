@@ -98,3 +98,139 @@ extern "C" ecl_status ecl_minplus_peak(int32_t variant, double* ops_per_s) {
   *ops_per_s = 2.0 * updates / (best_ms * 1e-3);
   return ECL_OK;
 }
+
+// ---- dependency-hop latency ----------------------------------------------------
+//
+// One hop of a dependency chain: a warp stores a value another warp is
+// polling for, and that warp's own next store follows.  Two warps ping-pong a
+// counter `iters` times each way; one hop is the event-timed launch divided
+// by the 2 * iters hops.  Variant 0: two CTAs on two SMs (one block per SM by
+// their shared-memory size) through an L2 word, waiting the way GC's pull
+// waits (relaxed device-scope loads, __nanosleep back-off from 32 to 512 ns).
+// Variant 1: the same with a bare spin.  Variant 2: two warps of one CTA
+// through a shared-memory word, waiting the way GC's core waits.  Every wait
+// is bounded; a wait that runs out sets *failed and both sides stop.
+
+namespace ecl {
+namespace {
+
+constexpr unsigned long long kHopWaitNs = 2000000000ull;  // a wait gives up after 2 s
+
+__device__ __forceinline__ unsigned long long hop_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+template <int V>
+__device__ __forceinline__ bool hop_wait(const unsigned* p, unsigned want, const unsigned* stop) {
+  unsigned nap = 32;
+  const unsigned long long t0 = hop_now();
+  for (unsigned spins = 0;; spins++) {
+    unsigned cur;
+    if (V == 2)
+      cur = cuda::atomic_ref<unsigned, cuda::thread_scope_block>(*const_cast<unsigned*>(p)).load(
+          cuda::memory_order_relaxed);
+    else
+      cur = dev::ld(p);
+    if (cur == want) return true;
+    if ((spins & 255u) == 255u && (dev::ld(stop) != 0 || hop_now() - t0 > kHopWaitNs)) return false;
+    if (V == 0) {
+      __nanosleep(nap);
+      nap = min(nap * 2, 512u);
+    } else if (V == 2 && spins > 8) {
+      __nanosleep(32);
+    }
+  }
+}
+
+template <int V>
+__global__ void hop_kernel(unsigned* __restrict__ word, unsigned* __restrict__ failed, int iters) {
+  __shared__ unsigned s_word;
+  const int side = (V == 2) ? (int)(threadIdx.x >> 5) : (int)blockIdx.x;  // 0 or 1
+  if (V == 2 && threadIdx.x == 0) s_word = 0;
+  if (V == 2) __syncthreads();
+  if ((threadIdx.x & 31) != 0) return;
+  unsigned* p = (V == 2) ? &s_word : word;
+  for (int i = 0; i < iters; i++) {
+    const unsigned mine = 2u * (unsigned)i + (unsigned)side + 1u;  // side 0 writes odd, side 1 even values
+    if (mine > 1 && !hop_wait<V>(p, mine - 1, failed)) {
+      dev::st(failed, 1u);
+      return;
+    }
+    if (V == 2)
+      cuda::atomic_ref<unsigned, cuda::thread_scope_block>(*p).store(mine, cuda::memory_order_relaxed);
+    else
+      dev::st(p, mine);
+  }
+}
+
+}  // namespace
+}  // namespace ecl
+
+extern "C" ecl_status ecl_hop_latency(int32_t variant, double* ns_per_hop) {
+  if (!ns_per_hop || variant < 0 || variant > 2) {
+    set_last_error_msg("ecl_hop_latency: variant must be 0, 1 or 2 and ns_per_hop non-null");
+    return ECL_ERR_INVALID_ARG;
+  }
+  *ns_per_hop = 0.0;
+  DeviceInfo di;
+  const ecl_status st = current_device(&di);
+  if (st != ECL_OK) return st;
+  const int iters = 20000;
+  unsigned* buf = nullptr;  // [0] the L2 word, [32] the failure flag (separate 128-byte lines)
+  ECL_CUDA_TRY(cudaMalloc(&buf, 64 * sizeof(unsigned)));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t err = cudaEventCreate(&e0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e1);
+  // more than half an SM's shared memory per block: the two blocks of the L2
+  // variants cannot share an SM
+  const size_t smem = di.smem_optin / 2 + 1024;
+  if (err == cudaSuccess && variant != 2) {
+    err = cudaFuncSetAttribute(variant == 0 ? hop_kernel<0> : hop_kernel<1>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  float best_ms = 0.f;
+  unsigned failed = 0;
+  for (int rep = 0; rep < 3 && err == cudaSuccess && !failed; rep++) {  // rep 0 warms up
+    err = cudaMemset(buf, 0, 64 * sizeof(unsigned));
+    if (err != cudaSuccess) break;
+    cudaEventRecord(e0, 0);
+    if (variant == 2) {
+      ECL_LAUNCH(hop_kernel<2>, 1, 64, 0, 0, buf, buf + 32, iters);
+    } else {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(2);
+      cfg.blockDim = dim3(32);
+      cfg.dynamicSmemBytes = smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;  // both blocks resident at once
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      err = variant == 0 ? cudaLaunchKernelEx(&cfg, hop_kernel<0>, buf, buf + 32, iters)
+                         : cudaLaunchKernelEx(&cfg, hop_kernel<1>, buf, buf + 32, iters);
+      count_launch();
+      if (err != cudaSuccess) break;
+    }
+    cudaEventRecord(e1, 0);
+    err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (err == cudaSuccess) err = cudaMemcpy(&failed, buf + 32, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    if (rep > 0 && (best_ms == 0.f || ms < best_ms)) best_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  if (err != cudaSuccess) {
+    set_last_error("ecl_hop_latency", err);
+    return ECL_ERR_CUDA;
+  }
+  if (failed) {
+    set_last_error_msg("ecl_hop_latency: a wait ran out of its bound");
+    return ECL_ERR_NO_CONVERGENCE;
+  }
+  *ns_per_hop = best_ms * 1e6 / (2.0 * iters);
+  return ECL_OK;
+}

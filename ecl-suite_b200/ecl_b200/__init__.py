@@ -101,6 +101,9 @@ _sig("ecl_last_error", C.c_char_p, [])
 _sig("ecl_workspace_bytes", C.c_size_t, [C.c_int, _I32, _I32])
 _sig("ecl_kernel_launches", C.c_uint64, [])
 _sig("ecl_minplus_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double)])
+_sig("ecl_hop_latency", C.c_int, [C.c_int32, C.POINTER(C.c_double)])
+_sig("ecl_gc_critical_path", C.c_int, [_PV, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32),
+                                        C.POINTER(C.c_int32), C.POINTER(C.c_double)])
 _sig("ecl_cc", C.c_int, [_PV, _VP, _PO])
 _sig("ecl_mis", C.c_int, [_PV, _VP, _PO])
 _sig("ecl_gc", C.c_int, [_PV, _VP, _PO])
@@ -118,7 +121,7 @@ _sig("ecl_gen_er", C.c_int, [_I32, _F64, _U64, _I32, _U64, _I32, _I32, _PG])
 # Every symbol that include/ecl_b200.h declares (checked by the CPU tests).
 EXPORTED = [
     "ecl_abi_version", "ecl_status_string", "ecl_last_error", "ecl_workspace_bytes", "ecl_kernel_launches",
-    "ecl_minplus_peak", "ecl_set_tune", "ecl_get_tune",
+    "ecl_minplus_peak", "ecl_hop_latency", "ecl_gc_critical_path", "ecl_set_tune", "ecl_get_tune",
     "ecl_cc", "ecl_mis", "ecl_gc", "ecl_mst", "ecl_scc", "ecl_apsp",
     "ecl_compute_cc", "ecl_compute_mis", "ecl_compute_gc", "ecl_compute_mst", "ecl_compute_scc", "ecl_compute_apsp",
     "ecl_graph_read", "ecl_graph_write", "ecl_graph_free", "ecl_graph_validate",
@@ -374,6 +377,24 @@ def minplus_peak(variant: int = 0) -> float:
     v = C.c_double(0.0)
     _check(lib.ecl_minplus_peak(variant, C.byref(v)), "ecl_minplus_peak")
     return float(v.value)
+
+
+def hop_latency(variant: int = 0) -> float:
+    """Measured ns of one dependency hop (0: L2 with GC's back-off polling,
+    1: L2 with a bare spin, 2: shared memory between two warps of a CTA)."""
+    v = C.c_double(0.0)
+    _check(lib.ecl_hop_latency(variant, C.byref(v)), "ecl_hop_latency")
+    return float(v.value)
+
+
+def gc_critical_path(g: "Graph", core_ranks: int = 0, hop_core_ns: float = 0.0, hop_rest_ns: float = 0.0):
+    """GC's longest dependency chain of a host graph: (hops, hops inside the
+    shared-memory core, the chain's time with the given hop costs in ns)."""
+    v = g.view()
+    h, hc, t = C.c_int32(0), C.c_int32(0), C.c_double(0.0)
+    _check(lib.ecl_gc_critical_path(C.byref(v), core_ranks, hop_core_ns, hop_rest_ns, C.byref(h), C.byref(hc),
+                                    C.byref(t)), "ecl_gc_critical_path")
+    return int(h.value), int(hc.value), float(t.value)
 
 
 # ---- batched engine (include/ecl_batch.h) ------------------------------------------

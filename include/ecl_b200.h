@@ -127,6 +127,21 @@ uint64_t ecl_kernel_launches(void);
  * APSP kernels issue, variant 1 a separate add and min.  No counterpart in the
  * reference. */
 ecl_status ecl_minplus_peak(int32_t variant, double* ops_per_s);
+/* Measured time of one dependency hop on the current device, in ns: a warp
+ * stores a value another warp polls for, and that warp's next store follows.
+ * variant 0: between two SMs through an L2 word, polled the way GC's pull
+ * polls (sleep back-off); 1: the same with a bare spin; 2: between two warps
+ * of one CTA through shared memory, polled the way GC's core polls.  The
+ * latency denominators of GC's roofline.  No counterpart in the reference. */
+ecl_status ecl_hop_latency(int32_t variant, double* ns_per_hop);
+/* GC's critical path, computed on the host for a host graph: *hops = the
+ * longest chain of higher-priority dependencies (ECL-GC-atomic.cu:102
+ * priorities), *hops_core = its part inside the first min(long rows,
+ * core_ranks) ranks (0 = the default core size), and *path_ns = the longest
+ * chain's time when a hop into the core costs hop_core_ns and any other hop
+ * hop_rest_ns -- the latency bound of ecl_gc.  No counterpart in the reference. */
+ecl_status ecl_gc_critical_path(const ecl_graph_view* g, int32_t core_ranks, double hop_core_ns, double hop_rest_ns,
+                                int32_t* hops, int32_t* hops_core, double* path_ns);
 
 /* ---- solvers ------------------------------------------------------------------ */
 
