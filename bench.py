@@ -264,9 +264,8 @@ def phase_bytes(code, phase, n, m):
         ("mst", 2): 16 * n,
         ("mst", 3): 4 * (n + 1) + 8 * m + 4 * n,   # heavy scan: CSR + weights + roots
         ("mst", 4): 16 * n,
-        ("scc", 0): csr + 12 * n,
-        ("scc", 1): csr + 4 * n,
-        ("scc", 2): 8 * m + 12 * n,
+        ("scc", 0): csr + 4 * n + 8 * m,           # mark: CSR read, flags, the 8-byte edge list written
+        ("scc", 1): 8 * m + 12 * n,                # solve: one sweep of the edge list, io words and labels
     }
     return table[(code, phase)] if (code, phase) in table else csr
 
@@ -278,7 +277,7 @@ PHASE_NAMES = {
     "gc": ["gc_keys+init+chunks", "radix_sort", "gc_core", "gc_pull"],
     "mst": ["mst_init+threshold", "mst_scan<light>+chunks", "mst_boruvka(light)", "mst_scan<heavy>+chunks",
             "mst_boruvka(heavy)"],
-    "scc": ["scc_mark+chunks", "scc_build+chunks", "scc_solve"],
+    "scc": ["scc_mark+chunks", "scc_solve"],
     "apsp": ["apsp_fill+edges", "apsp_panels+update"],
 }
 

@@ -412,19 +412,38 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
 // entry of a core row is itself a core vertex (it has a smaller rank), so a
 // core row never waits on global memory.  Two small launches first rewrite
 // the core rows' entries in nl2 from vertex ids to ranks (rank[] is the
-// inverse of the order over the core), so the core reads its entries with
-// coalesced loads and looks their colours up in shared memory.  gc_pull then
-// starts its long rows after the core.
+// inverse of the order over the core) and record each core rank's row
+// (start, length, vertex).
+//
+// One SM has to stream all core rows (16.6 M entries for the first 32k ranks
+// of R-MAT-22), and a warp that fetched each row with its own loads paid a
+// dependent L2 round trip per 128 entries.  Instead every warp stages its
+// rows through two shared-memory buffers with bulk asynchronous copies
+// (cp.async.bulk, completion counted on an mbarrier): while it colours one
+// segment of a row, the next segment -- of this row or of its next row -- is
+// already on its way, and the scan itself reads shared memory only.  Colours
+// are 16-bit words (0xffff = not yet coloured; a core colour is at most the
+// row's length, below 2^15).
 constexpr int kCoreThreads = 1024;
 constexpr int kCoreWarps = kCoreThreads / 32;
-constexpr int kCorePend = 512;          // per-warp list of undecided entries
+constexpr int kCorePend = 512;          // per-warp list of undecided entries (ranks)
 constexpr int kCoreBatch = 4;           // entries per lane whose loads are in flight together
 constexpr int kCoreDefault = 32768;     // default core size (ranks)
-constexpr int kCoreMax = 36864;         // shared memory bound: colours + per-warp bitmaps and lists
+constexpr int kCoreMax = 36864;         // shared memory bound
+constexpr int kSegBuf = 384;            // entries per staging buffer
+constexpr int kSeg = 376;               // row entries staged at a time (plus <= 3 + 3 of 16-byte alignment slack)
+constexpr unsigned kUncoloured = 0xffffu;
 
+// Dynamic shared memory of the core CTA: colours (16-bit, per rank), then per
+// warp two mbarriers, two staging buffers, a 2048-colour bitmap and the list
+// of undecided entries.
+__host__ __device__ constexpr size_t gc_core_colour_bytes(int cap) { return ((size_t)cap * 2 + 15) & ~size_t(15); }
 __host__ __device__ constexpr size_t gc_core_smem(int cap) {
-  return sizeof(int) * ((size_t)cap + (size_t)kCoreWarps * (kMexWords + kCorePend));
+  return gc_core_colour_bytes(cap) +
+         (size_t)kCoreWarps * (2 * sizeof(unsigned long long) + 2 * kSegBuf * sizeof(int) + kMexWords * sizeof(unsigned) +
+                               kCorePend * sizeof(unsigned short));
 }
+static_assert(gc_core_smem(kCoreMax) <= 227 * 1024, "core shared memory over the per-block limit");
 
 // Core size of this solve: the long rows (a prefix of the order), at most cap.
 __device__ __forceinline__ int gc_core_size(const GCCtl* ctl, int cap) { return min(ld(&ctl->nbig), cap); }
@@ -437,33 +456,81 @@ __global__ void __launch_bounds__(kTPB) gc_core_rank(const int* __restrict__ ord
 }
 
 // Rewrites the higher-priority entries of every core row from vertex ids to
-// ranks, one warp per row.  Such an entry outranks its row, so its rank is
-// below the row's and inside the core.
+// ranks, one warp per row, and records the row: rowinfo[r] = (first entry,
+// length, vertex).  Such an entry outranks its row, so its rank is below the
+// row's and inside the core.
 __global__ void __launch_bounds__(kTPB) gc_core_translate(const int* __restrict__ nindex, int* __restrict__ nl2,
                                                           const int* __restrict__ hc, const int* __restrict__ order,
-                                                          const int* __restrict__ rank, const GCCtl* __restrict__ ctl,
-                                                          int cap) {
+                                                          const int* __restrict__ rank, int4* __restrict__ rowinfo,
+                                                          const GCCtl* __restrict__ ctl, int cap) {
   const int lane = threadIdx.x & 31;
   const int core = gc_core_size(ctl, cap);
   const int warp = (blockIdx.x * kTPB + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * kTPB) >> 5;
   for (int r = warp; r < core; r += nwarps) {
     const int v = __ldg(&order[r]);
-    const int b = __ldg(&nindex[v]), e = b + __ldg(&hc[v]);
-    for (int i = b + lane; i < e; i += 32) nl2[i] = __ldg(&rank[nl2[i]]);
+    const int b = __ldg(&nindex[v]), h = __ldg(&hc[v]);
+    for (int i = b + lane; i < b + h; i += 32) nl2[i] = __ldg(&rank[nl2[i]]);
+    if (lane == 0) rowinfo[r] = make_int4(b, h, v, 0);
   }
 }
 
-// Colour in shared memory of core rank q once it is published; -1 when the
-// wait gives up (2 s without the colour, or another error raised).
-__device__ __forceinline__ int gc_core_wait(const int* col_s, int q, Status* status) {
-  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
-  int c = bref(*const_cast<int*>(&col_s[q])).load(cuda::memory_order_relaxed);
-  if (c >= 0) return c;
+// ---- shared-memory and bulk-copy primitives (CTA-local, inline PTX) ----
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// 16-bit colour words: relaxed CTA-scope atomic loads and stores.
+__device__ __forceinline__ unsigned col_ld(const unsigned short* p) {
+  unsigned short v;
+  asm volatile("ld.relaxed.cta.shared.u16 %0, [%1];" : "=h"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void col_st(unsigned short* p, unsigned v) {
+  asm volatile("st.relaxed.cta.shared.u16 [%0], %1;" ::"r"(smem_u32(p)), "h"((unsigned short)v) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Starts a bulk copy of `bytes` (a multiple of 16, both ends 16-byte aligned)
+// from global src into shared dst, completing on bar.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier generic reads of dst come first
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for the phase `parity` of bar (2 s); false when it ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = gc_now();
   for (unsigned spins = 1;; spins++) {
-    c = bref(*const_cast<int*>(&col_s[q])).load(cuda::memory_order_relaxed);
-    if (c >= 0) return c;
+    if (mbar_test(bar, parity)) return true;
+    if ((spins & 255u) == 0 && gc_now() - t0 > kStallNs) return false;
+  }
+}
+
+// Colour of core rank q once it is published; -1 when the wait gives up (2 s
+// without the colour, or another error raised).
+__device__ __forceinline__ int gc_core_wait(const unsigned short* col_s, int q, Status* status) {
+  unsigned c = col_ld(&col_s[q]);
+  if (c != kUncoloured) return (int)c;
+  const unsigned long long t0 = gc_now();
+  for (unsigned spins = 1;; spins++) {
+    c = col_ld(&col_s[q]);
+    if (c != kUncoloured) return (int)c;
     if ((spins & 1023u) == 0 && (gc_now() - t0 > kStallNs || ld(&status->code) != 0)) {
       raise(status, ECL_ERR_NO_CONVERGENCE, q);
       return -1;
@@ -474,49 +541,38 @@ __device__ __forceinline__ int gc_core_wait(const int* col_s, int q, Status* sta
   }
 }
 
-// Colour of core rank r whose entries (ranks) are nl2[wb, we): the smallest
-// colour none of them uses, by windows of 2048 colours.  One non-blocking
-// pass files the entries not coloured yet in `pend`; then each lane waits on
-// one listed entry at a time.  An entry outside [0, r) is not a
-// higher-priority core vertex: ECL_ERR_BAD_GRAPH.  Returns -1 on a stall.
-// All lanes call.
-__device__ int gc_core_row(int r, int wb, int we, const int* nl2, const int* col_s, unsigned* bits, int* pend,
-                           Status* status) {
-  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
+// Colour of core rank r whose entries (ranks) are nl2[wb, we), for colours
+// from `off0` on, read straight from global memory: the fallback for a row
+// whose first 2048 colours are all taken by its neighbours.  -1 on a stall.
+__device__ int gc_core_row_global(int r, int wb, int we, int off0, const int* nl2, const unsigned short* col_s,
+                                  unsigned* bits, unsigned short* pend, Status* status) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1;
-  for (int off = 0;; off += 32 * kMexWords) {
+  for (int off = off0;; off += 32 * kMexWords) {
     bits[lane] = 0;
     bits[lane + 32] = 0;
     __syncwarp();
-    int cursor = wb;
-    while (cursor < we) {
+    for (int i0 = wb; i0 < we; i0 += 32 * kCoreBatch) {
       int np = 0;
-      int i0 = cursor;
-      for (; i0 < we && np + 32 * kCoreBatch <= kCorePend; i0 += 32 * kCoreBatch) {
-        int q[kCoreBatch], c[kCoreBatch];
+      int q[kCoreBatch];
 #pragma unroll
-        for (int k = 0; k < kCoreBatch; k++) {
-          const int i = i0 + 32 * k + lane;
-          q[k] = i < we ? __ldg(&nl2[i]) : -1;
-          if (i < we && (unsigned)q[k] >= (unsigned)r) {
-            raise(status, ECL_ERR_BAD_GRAPH, r);
-            q[k] = -1;
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kCoreBatch; k++)
-          c[k] = q[k] >= 0 ? bref(*const_cast<int*>(&col_s[q[k]])).load(cuda::memory_order_relaxed) : 0;
-#pragma unroll
-        for (int k = 0; k < kCoreBatch; k++) {
-          const bool undecided = q[k] >= 0 && c[k] < 0;
-          if (q[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
-          const unsigned ub = __ballot_sync(kFull, undecided);
-          if (undecided) pend[np + __popc(ub & lt)] = q[k];
-          np += __popc(ub);
+      for (int k = 0; k < kCoreBatch; k++) {
+        const int i = i0 + 32 * k + lane;
+        q[k] = i < we ? __ldg(&nl2[i]) : -1;
+        if (i < we && (unsigned)q[k] >= (unsigned)r) {
+          raise(status, ECL_ERR_BAD_GRAPH, r);
+          q[k] = -1;
         }
       }
-      cursor = i0;
+#pragma unroll
+      for (int k = 0; k < kCoreBatch; k++) {
+        const unsigned c = q[k] >= 0 ? col_ld(&col_s[q[k]]) : 0u;
+        const bool undecided = q[k] >= 0 && c == kUncoloured;
+        if (q[k] >= 0 && !undecided) gc_mark(bits, (int)c, off);
+        const unsigned ub = __ballot_sync(kFull, undecided);
+        if (undecided) pend[np + __popc(ub & lt)] = (unsigned short)q[k];
+        np += __popc(ub);
+      }
       __syncwarp();
       bool stalled = false;
       for (int j = lane; j < np; j += 32) {
@@ -545,31 +601,198 @@ __device__ int gc_core_row(int r, int wb, int we, const int* nl2, const int* col
   }
 }
 
+// Per-warp staging of row segments: two buffers, each with its mbarrier and
+// the parity of its next phase.  A segment is (first entry in nl2, length <=
+// kSeg); the copy starts at the 16-byte boundary at or below the first entry
+// and ends at the one at or above its end (nl2 holds 4 spare entries past m,
+// so the rounding never leaves the array).
+struct CoreStage {
+  int* buf[2];
+  unsigned long long* bar[2];
+  unsigned parity[2] = {0u, 0u};
+  int first[2] = {-1, -1};  // segment in each buffer (-1: none in flight)
+  int len[2] = {0, 0};
+
+  __device__ __forceinline__ void issue(int b, const int* nl2, int f, int l) {
+    first[b] = f;
+    len[b] = l;
+    if ((threadIdx.x & 31) == 0) {
+      const int a = f & ~3, e = (f + l + 3) & ~3;
+      bulk_load(buf[b], nl2 + a, 4u * (unsigned)(e - a), bar[b]);
+    }
+  }
+  // Waits for buffer b's copy; the segment's entries then start at
+  // buf[b] + offset(b).  False when the wait ran out.
+  __device__ __forceinline__ bool wait(int b) {
+    const bool ok = mbar_wait(bar[b], parity[b]);
+    if (ok) parity[b] ^= 1u;  // a copy that did not land stays listed for drain()
+    return ok;
+  }
+  __device__ __forceinline__ int offset(int b) const { return first[b] & 3; }
+  // Bounded wait for every copy still in flight (before leaving on an error).
+  __device__ __forceinline__ void drain() {
+    for (int b = 0; b < 2; b++)
+      if (first[b] >= 0) {
+        if (mbar_wait(bar[b], parity[b])) parity[b] ^= 1u;
+        first[b] = -1;
+      }
+  }
+};
+
 // One CTA colours the core: rank r goes to warp r mod 32, each warp takes its
 // ranks in increasing order (the warp holding the lowest uncoloured rank can
 // always finish it), and every colour is published to shared memory for the
-// core and to color[] for gc_pull.
-__global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict__ nindex, const int* __restrict__ nl2,
-                                                           const int* __restrict__ hc, const int* __restrict__ order,
+// core and to color[] for gc_pull.  A warp's rows are a stream of segments;
+// while one segment is scanned from shared memory the next is being copied.
+__global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict__ nl2, const int4* __restrict__ rowinfo,
                                                            int* __restrict__ color, const GCCtl* __restrict__ ctl,
                                                            int cap, Status* __restrict__ status) {
-  using bref = cuda::atomic_ref<int, cuda::thread_scope_block>;
-  extern __shared__ int s_core[];
+  extern __shared__ __align__(16) unsigned char s_core[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1;
   const int core = gc_core_size(ctl, cap);
-  int* col_s = s_core;
-  unsigned* bits = reinterpret_cast<unsigned*>(s_core + cap) + warp * kMexWords;
-  int* pend = s_core + cap + kCoreWarps * kMexWords + warp * kCorePend;
-  for (int r = threadIdx.x; r < core; r += kCoreThreads) bref(col_s[r]).store(-1, cuda::memory_order_relaxed);
+  unsigned short* col_s = reinterpret_cast<unsigned short*>(s_core);
+  unsigned char* wbase = s_core + gc_core_colour_bytes(cap) +
+                         (size_t)warp * (2 * sizeof(unsigned long long) + 2 * kSegBuf * sizeof(int) +
+                                         kMexWords * sizeof(unsigned) + kCorePend * sizeof(unsigned short));
+  CoreStage stg;
+  stg.bar[0] = reinterpret_cast<unsigned long long*>(wbase);
+  stg.bar[1] = stg.bar[0] + 1;
+  stg.buf[0] = reinterpret_cast<int*>(wbase + 2 * sizeof(unsigned long long));
+  stg.buf[1] = stg.buf[0] + kSegBuf;
+  unsigned* bits = reinterpret_cast<unsigned*>(stg.buf[1] + kSegBuf);
+  unsigned short* pend = reinterpret_cast<unsigned short*>(bits + kMexWords);
+  for (int r = threadIdx.x; r < core; r += kCoreThreads) col_st(&col_s[r], kUncoloured);
+  if (lane == 0) {
+    mbar_init(stg.bar[0]);
+    mbar_init(stg.bar[1]);
+    mbar_fence_init();
+  }
   __syncthreads();
-  for (int r = warp; r < core; r += kCoreWarps) {
-    const int v = __ldg(&order[r]);
-    const int wb = __ldg(&nindex[v]);
-    const int c = gc_core_row(r, wb, wb + __ldg(&hc[v]), nl2, col_s, bits, pend, status);
-    if (c < 0) return;
+
+  // Row j of this warp is rank warp + 32 j; lane L holds the row record of
+  // row jb + L (records are fetched 32 rows at a time).
+  int jb = -32;
+  int4 rec = make_int4(0, 0, -1, 0);
+  auto row_of = [&](int j) -> int4 {  // all lanes call
+    if ((j & ~31) != jb) {
+      jb = j & ~31;
+      const int r = warp + 32 * (jb + lane);
+      rec = r < core ? __ldg(&rowinfo[r]) : make_int4(0, 0, -1, 0);
+    }
+    const int src = j & 31;
+    return make_int4(__shfl_sync(kFull, rec.x, src), __shfl_sync(kFull, rec.y, src), __shfl_sync(kFull, rec.z, src),
+                     0);
+  };
+  const int nrows = core > warp ? (core - warp + kCoreWarps - 1) / kCoreWarps : 0;
+  int b = 0;  // buffer holding (or about to hold) the segment to scan next
+  for (int j = 0; j < nrows; j++) {
+    const int r = warp + kCoreWarps * j;
+    const int4 row = row_of(j);
+    const int wb = row.x, h = row.y, v = row.z;
+    bits[lane] = 0;
+    bits[lane + 32] = 0;
+    __syncwarp();
+    int np = 0;
+    bool stalled = false;
+    for (int off = 0; off < h && !stalled; off += kSeg) {
+      const int f = wb + off, l = min(kSeg, h - off);
+      if (stg.first[b] >= 0 && stg.first[b] != f) {  // a prefetch of another segment: cannot happen
+        raise(status, ECL_ERR_CUDA, r);
+        stalled = true;
+        break;
+      }
+      if (stg.first[b] != f) stg.issue(b, nl2, f, l);  // not prefetched
+      // prefetch what comes next: this row's next segment, or the first one
+      // of the warp's next row with entries (rows without any are skipped)
+      __syncwarp();  // buffer b ^ 1 was scanned by every lane
+      if (off + kSeg < h) {
+        stg.issue(b ^ 1, nl2, f + kSeg, min(kSeg, h - off - kSeg));
+      } else {
+        for (int jn = j + 1; jn < nrows; jn++) {
+          const int4 nx = row_of(jn);
+          if (nx.y > 0) {
+            stg.issue(b ^ 1, nl2, nx.x, min(kSeg, nx.y));
+            break;
+          }
+        }
+      }
+      if (!stg.wait(b)) {
+        raise(status, ECL_ERR_NO_CONVERGENCE, r);
+        stalled = true;
+        break;
+      }
+      const int* seg = stg.buf[b] + stg.offset(b);
+      stg.first[b] = -1;
+      // scan the staged entries: colours already published go into the
+      // bitmap, the others into the pending list
+      for (int i0 = 0; i0 < l; i0 += 32 * kCoreBatch) {
+        int q[kCoreBatch];
+        unsigned c[kCoreBatch];
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++) {
+          const int i = i0 + 32 * k + lane;
+          q[k] = i < l ? seg[i] : -1;
+          if (i < l && (unsigned)q[k] >= (unsigned)r) {
+            raise(status, ECL_ERR_BAD_GRAPH, r);
+            q[k] = -1;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++) c[k] = q[k] >= 0 ? col_ld(&col_s[q[k]]) : 0u;
+#pragma unroll
+        for (int k = 0; k < kCoreBatch; k++) {
+          const bool undecided = q[k] >= 0 && c[k] == kUncoloured;
+          if (q[k] >= 0 && !undecided) gc_mark(bits, (int)c[k], 0);
+          const unsigned ub = __ballot_sync(kFull, undecided);
+          if (undecided) pend[np + __popc(ub & lt)] = (unsigned short)q[k];
+          np += __popc(ub);
+        }
+      }
+      b ^= 1;
+      // resolve the pending entries once the list could not take another
+      // segment, and at the end of the row
+      if (np > kCorePend - kSeg || off + kSeg >= h) {
+        __syncwarp();
+        for (int jj = lane; jj < np && !stalled; jj += 32) {
+          const int cc = gc_core_wait(col_s, pend[jj], status);
+          if (cc < 0)
+            stalled = true;
+          else
+            gc_mark(bits, cc, 0);
+        }
+        stalled = __any_sync(kFull, stalled);
+        np = 0;
+        __syncwarp();
+      }
+    }
+    if (stalled) {
+      stg.drain();
+      return;
+    }
+    // the smallest colour of the first window the bitmap leaves free
+    __syncwarp();
+    const unsigned w0 = bits[lane], w1 = bits[lane + 32];
+    const unsigned f0 = __ballot_sync(kFull, w0 != ~0u), f1 = __ballot_sync(kFull, w1 != ~0u);
+    int c = -1;
+    if (f0) {
+      const int wi = __ffs(f0) - 1;
+      c = wi * 32 + __ffs(~__shfl_sync(kFull, w0, wi)) - 1;
+    } else if (f1) {
+      const int wi = __ffs(f1) - 1;
+      c = (wi + 32) * 32 + __ffs(~__shfl_sync(kFull, w1, wi)) - 1;
+    }
+    __syncwarp();
+    if (c < 0) {  // all 2048 first colours taken: scan the row again for the next windows
+      c = gc_core_row_global(r, wb, wb + h, 32 * kMexWords, nl2, col_s, bits, pend, status);
+      if (c < 0) {
+        stg.drain();
+        return;
+      }
+    }
     if (lane == 0) {
-      bref(col_s[r]).store(c, cuda::memory_order_relaxed);
+      col_st(&col_s[r], (unsigned)c);
       st(&color[v], c);
     }
     __syncwarp();
@@ -628,11 +851,12 @@ struct GCBufs {
   unsigned* sort_temp;
   unsigned* vhash;
   int2* chunks;
+  int4* rowinfo;
 };
 
 void gc_layout(Carve& c, int n, int m, GCBufs* b) {
   b->ctl = c.take<GCCtl>(1);
-  b->nl2 = c.take<int>((size_t)(m > 0 ? m : 1));
+  b->nl2 = c.take<int>((size_t)m + 4);  // 4 spare entries: the core's aligned bulk copies may round up into them
   b->hc = c.take<int>((size_t)n);
   b->keys0 = c.take<unsigned long long>((size_t)n);
   b->keys1 = c.take<unsigned long long>((size_t)n);
@@ -641,6 +865,7 @@ void gc_layout(Carve& c, int n, int m, GCBufs* b) {
   b->sort_temp = c.take<unsigned>(radix_temp_words((size_t)n));
   b->vhash = c.take<unsigned>((size_t)n);
   b->chunks = c.take<int2>(row_chunk_capacity(m, kMinChunk));
+  b->rowinfo = c.take<int4>((size_t)std::min(n, kCoreMax));
 }
 
 }  // namespace
@@ -693,10 +918,9 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   const int cap = std::min(std::min(dev.gc_core_ranks > 0 ? dev.gc_core_ranks : kCoreDefault, kCoreMax), g.n);
   int* rank = reinterpret_cast<int*>(b.keys0);
   ECL_LAUNCH(gc_core_rank, grid, kTPB, 0, stream, order, rank, b.ctl, cap);
-  ECL_LAUNCH(gc_core_translate, grid, kTPB, 0, stream, g.nindex, b.nl2, b.hc, order, rank, b.ctl, cap);
+  ECL_LAUNCH(gc_core_translate, grid, kTPB, 0, stream, g.nindex, b.nl2, b.hc, order, rank, b.rowinfo, b.ctl, cap);
   ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
-  ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, g.nindex, b.nl2, b.hc, order, color, b.ctl, cap,
-             status);
+  ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
   mark();
   ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
                                   cap, status));

@@ -21,7 +21,8 @@ bool tune_valid(const ecl_tune& t) {
   const bool chunk_ok = t.row_chunk == 0 || (t.row_chunk >= dev::kMinChunk && t.row_chunk <= dev::kMaxChunk &&
                                               (t.row_chunk & (t.row_chunk - 1)) == 0);
   return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 8 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
-         t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok;
+         t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok &&
+         (t.scc_sweep_batch == 0 || t.scc_sweep_batch == 1 || t.scc_sweep_batch == 2 || t.scc_sweep_batch == 4);
 }
 
 void apply_tune(DeviceInfo* d, const ecl_tune& t) {
@@ -30,6 +31,7 @@ void apply_tune(DeviceInfo* d, const ecl_tune& t) {
   d->gc_core_ranks = t.gc_core_ranks;
   d->row_lane_max = t.row_lane_max;
   d->row_chunk = t.row_chunk;
+  d->scc_sweep_batch = t.scc_sweep_batch;
 }
 
 void set_last_error(const char* where, cudaError_t e) {

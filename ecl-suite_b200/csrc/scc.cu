@@ -26,7 +26,8 @@
 //    plus two for the jumps io[in-max(v)] / io[out-max(w)] (both still valid
 //    bounds, so values travel many hops per sweep); a raise is a 32-bit
 //    atomic max on one half.  Trimmed vertices hold a DEAD word that every
-//    sweep skips.  Each lane keeps kSweepBatch edges' loads in flight;
+//    sweep skips.  Each lane keeps kSweepBatch edges' loads in flight (a
+//    launch knob: 1, 2 or 4; fewer edges a lane leave more lanes resident);
 //  * rounds after the first compact the surviving edges (the edges whose two
 //    ends share both values and are unresolved: io[v] == io[w]);
 //  * the final labels are written by the same launch (label = in-max).
@@ -172,12 +173,18 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
 
 // Word of a trimmed vertex: it is its own SCC, and sweeps skip its edges.
 constexpr unsigned long long kDead = ~0ull;
-// Edges per lane whose loads are issued together in a sweep.
-constexpr int kSweepBatch = 4;
+// Edges per lane whose loads are issued together in a sweep: a template
+// argument (1, 2 or 4), with the blocks per SM the register budget allows.
+constexpr int kSweepBatchDefault = 2;
+template <int kSweepBatch>
+struct SweepOcc {
+  static constexpr int blocks = kSweepBatch == 1 ? 8 : (kSweepBatch == 2 ? 6 : 4);
+};
 
 // Round 0 sweeps the CSR-position edge list of `m0` slots (dead slots have
 // x < 0); later rounds sweep the compacted survivors.
-__global__ void __launch_bounds__(kTPB, 4) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
+template <int kSweepBatch>
+__global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
                                                   const int* __restrict__ flags, unsigned long long* __restrict__ io,
                                                   int* __restrict__ label, SCCCtl* __restrict__ ctl,
                                                   SCCRound* __restrict__ rounds, int max_rounds,
@@ -354,8 +361,11 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   Carve c{ws};
   SCCBufs b;
   scc_layout(c, g.n, g.m, &b);
+  const int batch = dev.scc_sweep_batch > 0 ? dev.scc_sweep_batch : kSweepBatchDefault;
+  void (*solve)(int, int, int2*, int2*, const int*, unsigned long long*, int*, SCCCtl*, SCCRound*, int, Status*) =
+      batch == 1 ? scc_solve<1> : (batch == 4 ? scc_solve<4> : scc_solve<2>);
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, scc_solve, kTPB, 0) != cudaSuccess || occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
@@ -373,8 +383,8 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, vec,
              status);
   mark();
-  ECL_CUDA_TRY(launch_cooperative(scc_solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label,
-                                  b.ctl, b.rounds, max_rounds, status));
+  ECL_CUDA_TRY(launch_cooperative(solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label, b.ctl,
+                                  b.rounds, max_rounds, status));
   mark();
   return ECL_OK;
 }

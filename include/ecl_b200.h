@@ -93,6 +93,7 @@ typedef struct ecl_tune {
   int32_t row_lane_max;   /* CSR scans: rows of at most this many entries go to one lane, 0..32; 0 = per code */
   int32_t row_chunk;      /* CSR scans: rows longer than this are cut into chunks of this many entries;
                              0 = per code, else a power of two in 128..8192 */
+  int32_t scc_sweep_batch; /* SCC: edges per lane whose loads a sweep keeps in flight: 1, 2 or 4; 0 = 2 */
 } ecl_tune;
 
 /* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);
