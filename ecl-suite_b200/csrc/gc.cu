@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
           }
         }
       }
-      if (!stg.wait(b)) {
+      if (!__all_sync(kFull, stg.wait(b))) {  // every lane polls; the verdict is the warp's
         raise(status, ECL_ERR_NO_CONVERGENCE, r);
         stalled = true;
         break;
