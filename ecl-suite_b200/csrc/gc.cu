@@ -426,24 +426,34 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
 // row's length, below 2^15).
 constexpr int kCoreThreads = 1024;
 constexpr int kCoreWarps = kCoreThreads / 32;
-constexpr int kCorePend = 512;          // per-warp list of undecided entries (ranks)
 constexpr int kCoreBatch = 4;           // entries per lane whose loads are in flight together
-constexpr int kCoreDefault = 32768;     // default core size (ranks)
+constexpr int kCoreDefault = 4096;      // default core size (ranks): the measured best at R-MAT-22
 constexpr int kCoreMax = 36864;         // shared memory bound
-constexpr int kSegBuf = 384;            // entries per staging buffer
-constexpr int kSeg = 376;               // row entries staged at a time (plus <= 3 + 3 of 16-byte alignment slack)
+constexpr int kSegSlack = 8;            // a buffer holds a segment plus its 16-byte alignment slack
+constexpr int kSegBufMax = 2048;
 constexpr unsigned kUncoloured = 0xffffu;
+constexpr size_t kCoreSmemLimit = 227 * 1024;
 
 // Dynamic shared memory of the core CTA: colours (16-bit, per rank), then per
-// warp two mbarriers, two staging buffers, a 2048-colour bitmap and the list
-// of undecided entries.
+// warp two mbarriers, two staging buffers of `segbuf` entries, a 2048-colour
+// bitmap and a list of up to `segbuf` undecided entries (16-bit ranks).  The
+// buffers take what the colours leave: the smaller the core, the longer the
+// segments (a whole typical hub row in one copy).
 __host__ __device__ constexpr size_t gc_core_colour_bytes(int cap) { return ((size_t)cap * 2 + 15) & ~size_t(15); }
-__host__ __device__ constexpr size_t gc_core_smem(int cap) {
-  return gc_core_colour_bytes(cap) +
-         (size_t)kCoreWarps * (2 * sizeof(unsigned long long) + 2 * kSegBuf * sizeof(int) + kMexWords * sizeof(unsigned) +
-                               kCorePend * sizeof(unsigned short));
+__host__ __device__ constexpr size_t gc_core_warp_bytes(int segbuf) {
+  return 2 * sizeof(unsigned long long) + (size_t)segbuf * (2 * sizeof(int) + sizeof(unsigned short)) +
+         kMexWords * sizeof(unsigned);
 }
-static_assert(gc_core_smem(kCoreMax) <= 227 * 1024, "core shared memory over the per-block limit");
+__host__ __device__ constexpr int gc_core_segbuf(int cap) {
+  const size_t fixed = gc_core_colour_bytes(cap) + kCoreWarps * gc_core_warp_bytes(0);
+  const size_t per = (kCoreSmemLimit - fixed) / kCoreWarps / (2 * sizeof(int) + sizeof(unsigned short));
+  return (int)((per < (size_t)kSegBufMax ? per : (size_t)kSegBufMax) & ~size_t(7));
+}
+__host__ __device__ constexpr size_t gc_core_smem(int cap) {
+  return gc_core_colour_bytes(cap) + kCoreWarps * gc_core_warp_bytes(gc_core_segbuf(cap));
+}
+static_assert(gc_core_segbuf(kCoreMax) >= 256 && gc_core_smem(kCoreMax) <= kCoreSmemLimit,
+              "core shared memory over the per-block limit");
 
 // Core size of this solve: the long rows (a prefix of the order), at most cap.
 __device__ __forceinline__ int gc_core_size(const GCCtl* ctl, int cap) { return min(ld(&ctl->nbig), cap); }
@@ -603,7 +613,7 @@ __device__ int gc_core_row_global(int r, int wb, int we, int off0, const int* nl
 
 // Per-warp staging of row segments: two buffers, each with its mbarrier and
 // the parity of its next phase.  A segment is (first entry in nl2, length <=
-// kSeg); the copy starts at the 16-byte boundary at or below the first entry
+// segbuf - 8); the copy starts at the 16-byte boundary at or below the first entry
 // and ends at the one at or above its end (nl2 holds 4 spare entries past m,
 // so the rounding never leaves the array).
 struct CoreStage {
@@ -653,15 +663,15 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
   const unsigned lt = (1u << lane) - 1;
   const int core = gc_core_size(ctl, cap);
   unsigned short* col_s = reinterpret_cast<unsigned short*>(s_core);
-  unsigned char* wbase = s_core + gc_core_colour_bytes(cap) +
-                         (size_t)warp * (2 * sizeof(unsigned long long) + 2 * kSegBuf * sizeof(int) +
-                                         kMexWords * sizeof(unsigned) + kCorePend * sizeof(unsigned short));
+  const int segbuf = gc_core_segbuf(cap);
+  const int kSeg = segbuf - kSegSlack;  // row entries staged at a time
+  unsigned char* wbase = s_core + gc_core_colour_bytes(cap) + (size_t)warp * gc_core_warp_bytes(segbuf);
   CoreStage stg;
   stg.bar[0] = reinterpret_cast<unsigned long long*>(wbase);
   stg.bar[1] = stg.bar[0] + 1;
   stg.buf[0] = reinterpret_cast<int*>(wbase + 2 * sizeof(unsigned long long));
-  stg.buf[1] = stg.buf[0] + kSegBuf;
-  unsigned* bits = reinterpret_cast<unsigned*>(stg.buf[1] + kSegBuf);
+  stg.buf[1] = stg.buf[0] + segbuf;
+  unsigned* bits = reinterpret_cast<unsigned*>(stg.buf[1] + segbuf);
   unsigned short* pend = reinterpret_cast<unsigned short*>(bits + kMexWords);
   for (int r = threadIdx.x; r < core; r += kCoreThreads) col_st(&col_s[r], kUncoloured);
   if (lane == 0) {
@@ -753,7 +763,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
       b ^= 1;
       // resolve the pending entries once the list could not take another
       // segment, and at the end of the row
-      if (np > kCorePend - kSeg || off + kSeg >= h) {
+      if (np + kSeg > segbuf || off + kSeg >= h) {  // the list holds segbuf entries
         __syncwarp();
         for (int jj = lane; jj < np && !stalled; jj += 32) {
           const int cc = gc_core_wait(col_s, pend[jj], status);

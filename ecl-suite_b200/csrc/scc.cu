@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
 constexpr unsigned long long kDead = ~0ull;
 // Edges per lane whose loads are issued together in a sweep: a template
 // argument (1, 2 or 4), with the blocks per SM the register budget allows.
-constexpr int kSweepBatchDefault = 2;
+constexpr int kSweepBatchDefault = 1;  // the measured best at R-MAT-22 (2.16 ms vs 2.24 / 2.40)
 template <int kSweepBatch>
 struct SweepOcc {
   static constexpr int blocks = kSweepBatch == 1 ? 8 : (kSweepBatch == 2 ? 6 : 4);
