@@ -241,7 +241,7 @@ constexpr int kPend = 1024;                             // per-warp list of unde
 constexpr int kBatch = 16;                              // entries per lane whose loads are in flight together
 
 // Colour of u once it is published (bounded wait).  Returns -1 on a stall.
-__device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* status) {
+__device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* status, unsigned nap_cap = 512u) {
   int c = ld(&color[u]);
   if (c >= 0) return c;
   unsigned nap = 32, spins = 0;
@@ -252,7 +252,7 @@ __device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* s
       return -1;
     }
     __nanosleep(nap);
-    nap = min(nap * 2, 512u);
+    nap = min(nap * 2, nap_cap);
   }
   return c;
 }
@@ -274,7 +274,7 @@ __device__ __forceinline__ void gc_mark(unsigned* bits, int c, int off) {
 // step of 32 entries; the listed ones are resolved and the pass resumes where
 // it stopped, so every entry is read once by the pass.  Returns -1 on a
 // stall.  All lanes call.
-__device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend,
+__device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend, unsigned nap_cap,
                            Status* status) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1;
@@ -313,7 +313,7 @@ __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, uns
         __syncwarp();
         bool stalled = false;
         if (lane < cnt) {
-          const int c = gc_wait_colour(color, pend[lane], status);
+          const int c = gc_wait_colour(color, pend[lane], status, nap_cap);
           if (c < 0)
             stalled = true;
           else
@@ -812,7 +812,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
                                                 const int* __restrict__ hc, const int* __restrict__ order,
                                                 int* __restrict__ color, GCCtl* __restrict__ ctl, int core_cap,
-                                                Status* __restrict__ status) {
+                                                unsigned long_nap, Status* __restrict__ status) {
   __shared__ unsigned s_bits[kTPB / 32][kMexWords];
   __shared__ int s_pend[kTPB / 32][kPend];
   const int lane = threadIdx.x & 31;
@@ -833,7 +833,7 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   for (int r = gc_core_size(ctl, core_cap) + gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
-    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, status);
+    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
     if (c < 0) return;
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
@@ -932,8 +932,11 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
   ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
   mark();
+  // the long rows' polls back off to at most gc_poll_ns (they carry the
+  // dependency chain; the short rows keep 512 ns)
+  const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 512u;
   ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
-                                  cap, status));
+                                  cap, long_nap, status));
   mark();
   return ECL_OK;
 }

@@ -73,6 +73,7 @@ struct DeviceInfo {
   int row_lane_max = 0;   // degree bins of the CSR scans (0 = each scan's default)
   int row_chunk = 0;
   int scc_sweep_batch = 0;  // SCC: edges per lane in flight in a sweep (0 = default)
+  int gc_poll_ns = 0;       // GC pull: longest back-off of a long row's polls, ns (0 = default)
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }
