@@ -90,47 +90,50 @@ __device__ __forceinline__ void push_chunks_warp(const RowChunks& rc, int chunk,
 
 // Visits the entries [jb, je) of one row with the whole warp, four entries a
 // lane per call of f(j, u, valid) -- j[k] the entry index, u[k] = nlist[j[k]],
-// valid[k] whether that slot holds an entry; every lane calls f the same
-// number of times, so f may use warp collectives.  With `vec` (nlist 16-byte
-// aligned) the 16-byte-aligned middle of the row is read with one 16-byte
-// load a lane (4 consecutive entries; 128 entries a warp step) and only the
-// unaligned head and tail (at most 3 entries each) with 4-byte loads;
-// otherwise every entry is a 4-byte load, 32 consecutive entries per k.
+// valid[k] whether that slot holds an entry of the row; every lane calls f the
+// same number of times, so f may use warp collectives.  With `vec` (nlist
+// 16-byte aligned) the row is walked in 16-byte-aligned quads of entries, one
+// quad a lane and 128 entries a warp step, each read with a single 16-byte
+// load; the quads at the two ends of the row are masked to it (the entries of
+// the neighbouring rows they also hold are read but not used), and a quad that
+// would reach past the array's m entries is read entry by entry.  Without
+// `vec` every entry is a 4-byte load, 32 consecutive entries per k.
 template <class F>
-__device__ __forceinline__ void warp_row(int jb, int je, bool vec, const int* nlist, F&& f) {
+__device__ __forceinline__ void warp_row(int jb, int je, int m, bool vec, const int* nlist, F&& f) {
   const int lane = threadIdx.x & 31;
   int j[4], u[4];
   bool valid[4];
-  auto scalar = [&](int i0, int end) {
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      j[k] = i0 + 32 * k + lane;
-      valid[k] = j[k] < end;
-      u[k] = valid[k] ? __ldg(&nlist[j[k]]) : -1;
-    }
-    f(j, u, valid);
-  };
   if (!vec) {
-    for (int i0 = jb; i0 < je; i0 += 128) scalar(i0, je);
+    for (int i0 = jb; i0 < je; i0 += 128) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        j[k] = i0 + 32 * k + lane;
+        valid[k] = j[k] < je;
+        u[k] = valid[k] ? __ldg(&nlist[j[k]]) : -1;
+      }
+      f(j, u, valid);
+    }
     return;
   }
-  const int a = min(je, (jb + 3) & ~3);  // first 16-byte boundary in the row
-  const int z = max(a, je & ~3);         // last one
-  if (jb < a) scalar(jb, a);
-  for (int i0 = a; i0 < z; i0 += 128) {
-    const int j0 = i0 + 4 * lane;
-    const bool in = j0 < z;  // z - a is a multiple of 4: all four or none
-    int4 x = make_int4(-1, -1, -1, -1);
-    if (in) x = __ldg(reinterpret_cast<const int4*>(nlist + j0));
-    u[0] = x.x, u[1] = x.y, u[2] = x.z, u[3] = x.w;
+  for (int i0 = jb & ~3; i0 < je; i0 += 128) {
+    const int q = i0 + 4 * lane;  // this lane's quad [q, q + 4)
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      j[k] = j0 + k;
-      valid[k] = in;
+      j[k] = q + k;
+      valid[k] = j[k] >= jb && j[k] < je;
     }
+    if (q + 4 <= m && q < je) {
+      const int4 x = __ldg(reinterpret_cast<const int4*>(nlist + q));
+      u[0] = x.x, u[1] = x.y, u[2] = x.z, u[3] = x.w;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; k++) u[k] = valid[k] ? __ldg(&nlist[j[k]]) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (!valid[k]) u[k] = -1;
     f(j, u, valid);
   }
-  if (z < je) scalar(z, je);
 }
 
 // Warp-aggregated slot in an append-only list; every lane of the warp calls.

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
       const int wend = __shfl_sync(kFull, end, who);
       const unsigned long long wkv = __shfl_sync(kFull, kv, who);
       int wh = 0;
-      warp_row(wbeg, wend, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
+      warp_row(wbeg, wend, m, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
         int cls[kInitBatch];
         gc_class_batch(u, valid, wv, wkv, n, keys, status, cls);
 #pragma unroll
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kTPB) gc_init(int n, int m, const int* __restr
   }
 }
 
-__global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restrict__ nindex,
+__global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, int m, const int* __restrict__ nindex,
                                                        const int* __restrict__ nlist, int* __restrict__ nl2,
                                                        int* __restrict__ hc, RowChunks rc, int chunk, bool vec,
                                                        const unsigned long long* __restrict__ keys,
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, const int* __restr
     const int beg = __ldg(&nindex[v]), end = __ldg(&nindex[v + 1]);
     const int stop = min(r.y + chunk, end);
     const unsigned long long kv = __ldg(&keys[n - 1 - v]);
-    warp_row(r.y, stop, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
+    warp_row(r.y, stop, m, vec, nlist, [&](const int(&)[4], const int (&u)[4], const bool (&valid)[4]) {
       int cls[kInitBatch];
       gc_class_batch(u, valid, v, kv, n, keys, status, cls);
       unsigned bh[kInitBatch];
@@ -430,7 +430,7 @@ constexpr int kCoreBatch = 4;           // entries per lane whose loads are in f
 constexpr int kCoreDefault = 4096;      // default core size (ranks): the measured best at R-MAT-22
 constexpr int kCoreMax = 36864;         // shared memory bound
 constexpr int kSegSlack = 8;            // a buffer holds a segment plus its 16-byte alignment slack
-constexpr int kSegBufMax = 2048;
+constexpr int kSegBufMax = 384;  // longer segments measured slower (one copy's latency per row is exposed)
 constexpr unsigned kUncoloured = 0xffffu;
 constexpr size_t kCoreSmemLimit = 227 * 1024;
 
@@ -916,9 +916,9 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   }
   // the priority keys first: gc_init compares neighbours by them
   ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
-  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0;  // 16-byte row loads
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && !dev.row_scalar;  // 16-byte row loads
   ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, vec, b.keys0, status);
-  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, vec, b.keys0,
+  ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, vec, b.keys0,
              status);
   mark();
   const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);

@@ -226,15 +226,15 @@ __device__ __forceinline__ void mst_emit_batch(int j0, int stride, int jend, boo
   }
 }
 
-// Emits the worklist entries of one warp-walked row segment [jb, je) of v:
-// the unaligned head (up to 3 entries) and tail go through mst_emit_batch;
-// the 16-byte-aligned middle is read with one 16-byte load of nlist and one
-// of eweight per lane (4 consecutive entries a lane), so a warp step covers
-// 128 entries with two load instructions instead of eight.  vec = false
-// (nlist or eweight not 16-byte aligned) keeps the scalar loads throughout.
-// All lanes call.
+// Emits the worklist entries of one warp-walked row segment [jb, je) of v.
+// With `vec` (nlist and eweight 16-byte aligned) the segment is walked in
+// 16-byte-aligned quads of entries, one quad a lane (128 entries a warp
+// step): one 16-byte load of nlist and, when any of the quad's entries is a
+// v < u entry, one of eweight.  The quads at the segment's ends are masked to
+// it, and a quad reaching past the arrays' m entries is read entry by entry.
+// Without `vec` the scalar mst_emit_batch walks it.  All lanes call.
 template <bool kLight>
-__device__ __forceinline__ void mst_emit_row(int jb, int je, bool vec, int v, int rv, int n, const int* nlist,
+__device__ __forceinline__ void mst_emit_row(int jb, int je, int m, bool vec, int v, int rv, int n, const int* nlist,
                                              const int* eweight, int thr, const int* parent, Stage& stg, int4* wl,
                                              int* cnt, int cap, bool& overflow, Status* status) {
   const int lane = threadIdx.x & 31;
@@ -244,21 +244,30 @@ __device__ __forceinline__ void mst_emit_row(int jb, int je, bool vec, int v, in
                              overflow, status);
     return;
   }
-  const int a = min(je, (jb + 3) & ~3);  // first 16-byte boundary
-  const int z = max(a, je & ~3);         // last one
-  if (jb < a)
-    mst_emit_batch<kLight>(jb + lane, 32, a, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
-                           overflow, status);
-  for (int i0 = a; i0 < z; i0 += 4 * 32) {
-    const int j0 = i0 + 4 * lane;
-    const bool active = j0 < z;  // z - a is a multiple of 4: a lane's 4 entries are all in or all out
-    int u[4] = {-1, -1, -1, -1}, w[4] = {0, 0, 0, 0}, ru[4];
-    if (active) {
-      const int4 x = __ldg(reinterpret_cast<const int4*>(nlist + j0));
+  for (int i0 = jb & ~3; i0 < je; i0 += 4 * 32) {
+    const int q = i0 + 4 * lane;  // this lane's quad [q, q + 4)
+    const bool whole = q + 4 <= m && q < je;
+    bool valid[4];
+    int u[4], w[4] = {0, 0, 0, 0}, ru[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) valid[k] = q + k >= jb && q + k < je;
+    if (whole) {
+      const int4 x = __ldg(reinterpret_cast<const int4*>(nlist + q));
       u[0] = x.x, u[1] = x.y, u[2] = x.z, u[3] = x.w;
-      if (x.x > v || x.y > v || x.z > v || x.w > v) {
-        const int4 y = __ldg(reinterpret_cast<const int4*>(eweight + j0));
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; k++) u[k] = valid[k] ? __ldg(&nlist[q + k]) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+      if (!valid[k]) u[k] = -1;
+    if (u[0] > v || u[1] > v || u[2] > v || u[3] > v) {
+      if (whole) {
+        const int4 y = __ldg(reinterpret_cast<const int4*>(eweight + q));
         w[0] = y.x, w[1] = y.y, w[2] = y.z, w[3] = y.w;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) w[k] = u[k] > v ? __ldg(&eweight[q + k]) : 0;
       }
     }
 #pragma unroll
@@ -269,10 +278,10 @@ __device__ __forceinline__ void mst_emit_row(int jb, int je, bool vec, int v, in
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
-      const int j = j0 + k;
+      const int j = q + k;
       bool keep = false;
       int4 e = make_int4(0, 0, 0, 0);
-      if (active) {
+      if (valid[k]) {
         if ((unsigned)u[k] >= (unsigned)n) {
           raise(status, ECL_ERR_BAD_GRAPH, u[k]);
         } else if (u[k] > v) {
@@ -292,9 +301,6 @@ __device__ __forceinline__ void mst_emit_row(int jb, int je, bool vec, int v, in
       stg.push(keep, e, wl, cnt, cap, overflow);
     }
   }
-  if (z < je)
-    mst_emit_batch<kLight>(z + lane, 32, je, true, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap,
-                           overflow, status);
 }
 
 // More v<n entries than the worklist holds: an asymmetric graph flagged
@@ -349,7 +355,7 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
       const int wrv = __shfl_sync(kFull, rv, who);
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
-      mst_emit_row<kLight>(wbeg, wend, vec, wv, wrv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow,
+      mst_emit_row<kLight>(wbeg, wend, m, vec, wv, wrv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow,
                            status);
     }
   }
@@ -360,7 +366,8 @@ __global__ void __launch_bounds__(kTPB) mst_scan(int n, int m, const int* __rest
 }
 
 template <bool kLight>
-__global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict__ nindex, const int* __restrict__ nlist,
+__global__ void __launch_bounds__(kTPB) mst_chunks(int n, int m, const int* __restrict__ nindex,
+                                                   const int* __restrict__ nlist,
                                                    const int* __restrict__ eweight, int* __restrict__ parent,
                                                    int4* __restrict__ wl, int cap, MSTCtl* __restrict__ ctl,
                                                    const int2* __restrict__ chunks, int chunk_cap, int chunk,
@@ -378,7 +385,7 @@ __global__ void __launch_bounds__(kTPB) mst_chunks(int n, const int* __restrict_
     const int v = rec.x;
     const int end = min(rec.y + chunk, __ldg(&nindex[v + 1]));
     const int rv = kLight ? v : ld(&parent[v]);
-    mst_emit_row<kLight>(rec.y, end, vec, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow, status);
+    mst_emit_row<kLight>(rec.y, end, m, vec, v, rv, n, nlist, eweight, thr, parent, stg, wl, cnt, cap, overflow, status);
   }
   stg.flush(wl, cnt, cap, overflow);
   mst_overflow(overflow, status);
@@ -572,7 +579,8 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
   const int grid = dev.grid_blocks(kTPB);
   const Bins bins = bins_of(dev, kMstBins);
   // 16-byte row loads need 16-byte-aligned arrays (entries j = 0 mod 4 then are)
-  const bool vec = ((reinterpret_cast<uintptr_t>(g.nlist) | reinterpret_cast<uintptr_t>(g.eweight)) & 15) == 0;
+  const bool vec =
+      ((reinterpret_cast<uintptr_t>(g.nlist) | reinterpret_cast<uintptr_t>(g.eweight)) & 15) == 0 && !dev.row_scalar;
   if (total_dev) *total_dev = &b.ctl->total;
   ECL_CUDA_TRY(cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), stream));
   if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));
@@ -585,13 +593,13 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
       if (pass == 0) {
         ECL_LAUNCH(mst_scan<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, bins, vec, status);
-        ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
+        ECL_LAUNCH(mst_chunks<true>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
                    b.ctl, b.chunks, b.chunk_cap, bins.chunk, vec, status);
       } else {
         ECL_LAUNCH(mst_flatten, grid, kTPB, 0, stream, g.n, b.parent);
         ECL_LAUNCH(mst_scan<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA,
                    b.cap, b.ctl, b.chunks, bins, vec, status);
-        ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
+        ECL_LAUNCH(mst_chunks<false>, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, g.eweight, b.parent, b.wlA, b.cap,
                    b.ctl, b.chunks, b.chunk_cap, bins.chunk, vec, status);
       }
       mark();

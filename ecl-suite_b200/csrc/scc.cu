@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
       const int wbeg = __shfl_sync(kFull, beg, who);
       const int wend = __shfl_sync(kFull, end, who);
       bool wout = false;
-      warp_row(wbeg, wend, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
+      warp_row(wbeg, wend, m, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
         scc_mark_batch(valid, wv, w, j, n, flags, wl, wout, status);
       });
       if (__any_sync(kFull, wout) && lane == who) out = true;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark(int n, int m, const int* __rest
   }
 }
 
-__global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __restrict__ nindex,
+__global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, int m, const int* __restrict__ nindex,
                                                         const int* __restrict__ nlist, int* __restrict__ flags,
                                                         int2* __restrict__ wl, RowChunks rc, int chunk, bool vec,
                                                         Status* __restrict__ status) {
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(kTPB) scc_mark_chunks(int n, const int* __rest
     const int2 r = rc.rec[c];
     const int end = min(r.y + chunk, __ldg(&nindex[r.x + 1]));
     bool out = false;
-    warp_row(r.y, end, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
+    warp_row(r.y, end, m, vec, nlist, [&](const int (&j)[4], const int (&w)[4], const bool (&valid)[4]) {
       scc_mark_batch(valid, r.x, w, j, n, flags, wl, out, status);
     });
     if (__any_sync(kFull, out) && lane == 0) fetch_or(&flags[r.x], kHasOut);
@@ -378,9 +378,9 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
   const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
-  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0;  // 16-byte row loads
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && !dev.row_scalar;  // 16-byte row loads
   ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins, vec, status);
-  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, vec,
+  ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, vec,
              status);
   mark();
   ECL_CUDA_TRY(launch_cooperative(solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label, b.ctl,

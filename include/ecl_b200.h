@@ -95,6 +95,7 @@ typedef struct ecl_tune {
                              0 = per code, else a power of two in 128..8192 */
   int32_t scc_sweep_batch; /* SCC: edges per lane whose loads a sweep keeps in flight: 1, 2 or 4; 0 = 1 */
   int32_t gc_poll_ns;      /* GC: longest sleep between polls of a long row's dependency, 0..4096 ns; 0 = 512 */
+  int32_t row_scalar;      /* CSR scans: 1 = read rows with 4-byte loads only; 0 = 16-byte quads where aligned */
 } ecl_tune;
 
 /* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);
