@@ -274,6 +274,12 @@ __device__ __forceinline__ void gc_mark(unsigned* bits, int c, int off) {
 // step of 32 entries; the listed ones are resolved and the pass resumes where
 // it stopped, so every entry is read once by the pass.  Returns -1 on a
 // stall.  All lanes call.
+// kPollAll: instead of each lane blocking on one listed entry and the rest of
+// the list being re-checked after that, the warp re-reads the whole list of
+// undecided entries on every poll (all loads of a poll in flight together) and
+// sleeps between polls -- the row is done one poll after its last dependency
+// is coloured, with no second round trip for the entries past the first 32.
+template <bool kPollAll>
 __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend, unsigned nap_cap,
                            Status* status) {
   const int lane = threadIdx.x & 31;
@@ -309,7 +315,42 @@ __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, uns
       }
       cursor = i0;  // the list is full or the row is done: resolve, then resume here
       int cnt = np;
-      while (cnt > 0) {
+      if (kPollAll) {
+        unsigned nap = 32, polls = 0;
+        const unsigned long long t0 = gc_now();
+        while (cnt > 0) {
+          int kept = 0;
+          for (int j0 = 0; j0 < cnt; j0 += 32 * kBatch) {
+            int u[kBatch], c[kBatch];
+#pragma unroll
+            for (int k = 0; k < kBatch; k++) {
+              const int j = j0 + 32 * k + lane;
+              u[k] = j < cnt ? pend[j] : -1;
+            }
+#pragma unroll
+            for (int k = 0; k < kBatch; k++) c[k] = u[k] >= 0 ? ld(&color[u[k]]) : 0;
+            __syncwarp();  // every lane has read its slots before any is overwritten
+#pragma unroll
+            for (int k = 0; k < kBatch; k++) {
+              const bool still = u[k] >= 0 && c[k] < 0;
+              if (u[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
+              const unsigned sb = __ballot_sync(kFull, still);
+              if (still) pend[kept + __popc(sb & lt)] = u[k];  // index <= j0 + k*32: already read
+              kept += __popc(sb);
+            }
+          }
+          cnt = kept;
+          if (cnt == 0) break;
+          const bool give_up = ++polls > (1u << 24) || gc_now() - t0 > kStallNs || ld(&status->code) != 0;
+          if (__any_sync(kFull, give_up)) {
+            if (lane == 0) raise(status, ECL_ERR_NO_CONVERGENCE, pend[0]);
+            return -1;
+          }
+          __nanosleep(nap);
+          nap = min(nap * 2, nap_cap);
+        }
+      }
+      while (!kPollAll && cnt > 0) {
         __syncwarp();
         bool stalled = false;
         if (lane < cnt) {
@@ -809,6 +850,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
   }
 }
 
+template <bool kPollAll>
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
                                                 const int* __restrict__ hc, const int* __restrict__ order,
                                                 int* __restrict__ color, GCCtl* __restrict__ ctl, int core_cap,
@@ -833,7 +875,7 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   for (int r = gc_core_size(ctl, core_cap) + gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
-    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
+    const int c = gc_long_row<kPollAll>(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
     if (c < 0) return;
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
@@ -896,8 +938,9 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   Carve c{ws};
   GCBufs b;
   gc_layout(c, g.n, g.m, &b);
+  auto pull = dev.gc_poll_all ? gc_pull<true> : gc_pull<false>;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pull, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
@@ -935,7 +978,7 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   // the long rows' polls back off to at most gc_poll_ns (they carry the
   // dependency chain; the short rows keep 512 ns)
   const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 512u;
-  ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
+  ECL_CUDA_TRY(launch_cooperative(pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
                                   cap, long_nap, status));
   mark();
   return ECL_OK;

@@ -96,6 +96,7 @@ typedef struct ecl_tune {
   int32_t scc_sweep_batch; /* SCC: edges per lane whose loads a sweep keeps in flight: 1, 2 or 4; 0 = 1 */
   int32_t gc_poll_ns;      /* GC: longest sleep between polls of a long row's dependency, 0..4096 ns; 0 = 512 */
   int32_t row_scalar;      /* CSR scans: 1 = read rows with 4-byte loads only; 0 = 16-byte quads where aligned */
+  int32_t gc_poll_all;     /* GC: 1 = a long row re-reads all its undecided entries on every poll; 0 = one a lane */
 } ecl_tune;
 
 /* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);
