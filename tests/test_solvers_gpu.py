@@ -89,9 +89,9 @@ def test_gc_large_colour_windows(ecl, orc):
 def test_gc_core_size_does_not_change_colours(ecl, orc, core):
     """The leading ranks are coloured in one CTA's shared memory and the rest
     by the grid-wide pull; where the boundary lies (1, 7, 64 ranks, or the
-    default, which covers every long row of these graphs) changes no colour.
-    A 2100-clique forces colours past the first 2048-colour window inside the
-    core."""
+    default of 4096) changes no colour.  A 2100-clique (every vertex a long
+    row inside the default core) forces colours past the first 2048-colour
+    window there."""
     old = ecl.set_tune(gc_core_ranks=core)
     try:
         cases = list(sym_cases(ecl)) + [("rmat16", ecl.gen_rmat(16, 16, seed=3))]
