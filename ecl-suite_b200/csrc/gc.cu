@@ -274,12 +274,6 @@ __device__ __forceinline__ void gc_mark(unsigned* bits, int c, int off) {
 // step of 32 entries; the listed ones are resolved and the pass resumes where
 // it stopped, so every entry is read once by the pass.  Returns -1 on a
 // stall.  All lanes call.
-// kPollAll: instead of each lane blocking on one listed entry and the rest of
-// the list being re-checked after that, the warp re-reads the whole list of
-// undecided entries on every poll (all loads of a poll in flight together) and
-// sleeps between polls -- the row is done one poll after its last dependency
-// is coloured, with no second round trip for the entries past the first 32.
-template <bool kPollAll>
 __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend, unsigned nap_cap,
                            Status* status) {
   const int lane = threadIdx.x & 31;
@@ -315,42 +309,7 @@ __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, uns
       }
       cursor = i0;  // the list is full or the row is done: resolve, then resume here
       int cnt = np;
-      if (kPollAll) {
-        unsigned nap = 32, polls = 0;
-        const unsigned long long t0 = gc_now();
-        while (cnt > 0) {
-          int kept = 0;
-          for (int j0 = 0; j0 < cnt; j0 += 32 * kBatch) {
-            int u[kBatch], c[kBatch];
-#pragma unroll
-            for (int k = 0; k < kBatch; k++) {
-              const int j = j0 + 32 * k + lane;
-              u[k] = j < cnt ? pend[j] : -1;
-            }
-#pragma unroll
-            for (int k = 0; k < kBatch; k++) c[k] = u[k] >= 0 ? ld(&color[u[k]]) : 0;
-            __syncwarp();  // every lane has read its slots before any is overwritten
-#pragma unroll
-            for (int k = 0; k < kBatch; k++) {
-              const bool still = u[k] >= 0 && c[k] < 0;
-              if (u[k] >= 0 && c[k] >= 0) gc_mark(bits, c[k], off);
-              const unsigned sb = __ballot_sync(kFull, still);
-              if (still) pend[kept + __popc(sb & lt)] = u[k];  // index <= j0 + k*32: already read
-              kept += __popc(sb);
-            }
-          }
-          cnt = kept;
-          if (cnt == 0) break;
-          const bool give_up = ++polls > (1u << 24) || gc_now() - t0 > kStallNs || ld(&status->code) != 0;
-          if (__any_sync(kFull, give_up)) {
-            if (lane == 0) raise(status, ECL_ERR_NO_CONVERGENCE, pend[0]);
-            return -1;
-          }
-          __nanosleep(nap);
-          nap = min(nap * 2, nap_cap);
-        }
-      }
-      while (!kPollAll && cnt > 0) {
+      while (cnt > 0) {
         __syncwarp();
         bool stalled = false;
         if (lane < cnt) {
@@ -471,23 +430,23 @@ constexpr int kCoreBatch = 4;           // entries per lane whose loads are in f
 constexpr int kCoreDefault = 4096;      // default core size (ranks): the measured best at R-MAT-22
 constexpr int kCoreMax = 36864;         // shared memory bound
 constexpr int kSegSlack = 8;            // a buffer holds a segment plus its 16-byte alignment slack
+constexpr int kCorePend = 1024;         // per-warp list of undecided entries (16-bit ranks)
 constexpr int kSegBufMax = 384;  // longer segments measured slower (one copy's latency per row is exposed)
 constexpr unsigned kUncoloured = 0xffffu;
 constexpr size_t kCoreSmemLimit = 227 * 1024;
 
 // Dynamic shared memory of the core CTA: colours (16-bit, per rank), then per
 // warp two mbarriers, two staging buffers of `segbuf` entries, a 2048-colour
-// bitmap and a list of up to `segbuf` undecided entries (16-bit ranks).  The
-// buffers take what the colours leave: the smaller the core, the longer the
-// segments (a whole typical hub row in one copy).
+// bitmap and a list of up to kCorePend undecided entries (16-bit ranks).  The
+// buffers take what the colours leave, up to kSegBufMax entries.
 __host__ __device__ constexpr size_t gc_core_colour_bytes(int cap) { return ((size_t)cap * 2 + 15) & ~size_t(15); }
 __host__ __device__ constexpr size_t gc_core_warp_bytes(int segbuf) {
-  return 2 * sizeof(unsigned long long) + (size_t)segbuf * (2 * sizeof(int) + sizeof(unsigned short)) +
-         kMexWords * sizeof(unsigned);
+  return 2 * sizeof(unsigned long long) + (size_t)segbuf * 2 * sizeof(int) + kMexWords * sizeof(unsigned) +
+         kCorePend * sizeof(unsigned short);
 }
 __host__ __device__ constexpr int gc_core_segbuf(int cap) {
   const size_t fixed = gc_core_colour_bytes(cap) + kCoreWarps * gc_core_warp_bytes(0);
-  const size_t per = (kCoreSmemLimit - fixed) / kCoreWarps / (2 * sizeof(int) + sizeof(unsigned short));
+  const size_t per = (kCoreSmemLimit - fixed) / kCoreWarps / (2 * sizeof(int));
   return (int)((per < (size_t)kSegBufMax ? per : (size_t)kSegBufMax) & ~size_t(7));
 }
 __host__ __device__ constexpr size_t gc_core_smem(int cap) {
@@ -804,7 +763,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
       b ^= 1;
       // resolve the pending entries once the list could not take another
       // segment, and at the end of the row
-      if (np + kSeg > segbuf || off + kSeg >= h) {  // the list holds segbuf entries
+      if (np + kSeg > kCorePend || off + kSeg >= h) {  // before the list could overflow, and at the row's end
         __syncwarp();
         for (int jj = lane; jj < np && !stalled; jj += 32) {
           const int cc = gc_core_wait(col_s, pend[jj], status);
@@ -850,7 +809,6 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
   }
 }
 
-template <bool kPollAll>
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
                                                 const int* __restrict__ hc, const int* __restrict__ order,
                                                 int* __restrict__ color, GCCtl* __restrict__ ctl, int core_cap,
@@ -875,7 +833,7 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   for (int r = gc_core_size(ctl, core_cap) + gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
-    const int c = gc_long_row<kPollAll>(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
+    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
     if (c < 0) return;
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
@@ -938,9 +896,8 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   Carve c{ws};
   GCBufs b;
   gc_layout(c, g.n, g.m, &b);
-  auto pull = dev.gc_poll_all ? gc_pull<true> : gc_pull<false>;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pull, kTPB, 0) != cudaSuccess || occ < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
   const int grid = dev.grid_blocks(kTPB);
@@ -959,7 +916,7 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   }
   // the priority keys first: gc_init compares neighbours by them
   ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
-  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && !dev.row_scalar;  // 16-byte row loads
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && dev.row_vec;  // 16-byte row loads
   ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, vec, b.keys0, status);
   ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, vec, b.keys0,
              status);
@@ -975,10 +932,10 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
   ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
   mark();
-  // the long rows' polls back off to at most gc_poll_ns (they carry the
-  // dependency chain; the short rows keep 512 ns)
-  const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 512u;
-  ECL_CUDA_TRY(launch_cooperative(pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
+  // the long rows' polls back off to at most gc_poll_ns, 128 ns by default
+  // (they carry the dependency chain; the short rows keep 512 ns)
+  const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 128u;
+  ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
                                   cap, long_nap, status));
   mark();
   return ECL_OK;

@@ -580,7 +580,7 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
   const Bins bins = bins_of(dev, kMstBins);
   // 16-byte row loads need 16-byte-aligned arrays (entries j = 0 mod 4 then are)
   const bool vec =
-      ((reinterpret_cast<uintptr_t>(g.nlist) | reinterpret_cast<uintptr_t>(g.eweight)) & 15) == 0 && !dev.row_scalar;
+      ((reinterpret_cast<uintptr_t>(g.nlist) | reinterpret_cast<uintptr_t>(g.eweight)) & 15) == 0 && dev.row_vec;
   if (total_dev) *total_dev = &b.ctl->total;
   ECL_CUDA_TRY(cudaMemsetAsync(b.ctl, 0, sizeof(MSTCtl), stream));
   if (g.m > 0) ECL_CUDA_TRY(cudaMemsetAsync(in_mst, 0, (size_t)g.m, stream));

@@ -74,8 +74,7 @@ struct DeviceInfo {
   int row_chunk = 0;
   int scc_sweep_batch = 0;  // SCC: edges per lane in flight in a sweep (0 = default)
   int gc_poll_ns = 0;       // GC pull: longest back-off of a long row's polls, ns (0 = default)
-  int row_scalar = 0;       // CSR scans: 1 = 4-byte row loads only (no 16-byte quads)
-  int gc_poll_all = 0;      // GC pull: 1 = a long row re-reads its whole pending list on every poll
+  int row_vec = 0;          // CSR scans: 1 = warp rows read in 16-byte quads where aligned
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }

@@ -378,7 +378,7 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
   const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
-  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && !dev.row_scalar;  // 16-byte row loads
+  const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && dev.row_vec;  // 16-byte row loads
   ECL_LAUNCH(scc_mark, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins, vec, status);
   ECL_LAUNCH(scc_mark_chunks, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.flags, b.wlA, rc, bins.chunk, vec,
              status);
