@@ -247,7 +247,10 @@ __device__ __forceinline__ int gc_wait_colour(const int* color, int u, Status* s
   unsigned nap = 32, spins = 0;
   const unsigned long long t0 = gc_now();
   while ((c = ld(&color[u])) < 0) {
-    if (++spins > (1u << 24) || gc_now() - t0 > kStallNs || ld(&status->code) != 0) {
+    // the stall checks every 64th poll: status->code is one word, and every
+    // polling lane of the grid reading it on every poll makes its L2 slice a
+    // hot spot that slows the colour polls themselves
+    if ((++spins & 63u) == 0 && (spins > (1u << 24) || gc_now() - t0 > kStallNs || ld(&status->code) != 0)) {
       raise(status, ECL_ERR_NO_CONVERGENCE, u);
       return -1;
     }
@@ -274,8 +277,8 @@ __device__ __forceinline__ void gc_mark(unsigned* bits, int c, int off) {
 // step of 32 entries; the listed ones are resolved and the pass resumes where
 // it stopped, so every entry is read once by the pass.  Returns -1 on a
 // stall.  All lanes call.
-__device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend, unsigned nap_cap,
-                           Status* status) {
+__device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, unsigned* bits, int* pend, int pend_cap,
+                           unsigned nap_cap, Status* status) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1;
   for (int off = 0;; off += 32 * kMexWords) {
@@ -289,7 +292,7 @@ __device__ int gc_long_row(int wb, int we, const int* nl2, const int* color, uns
       // kBatch entries per lane per step: all index loads, then all colour
       // loads, are issued before any result is used (one round trip per
       // 32 * kBatch entries instead of two per 32)
-      for (; i0 < we && np + 32 * kBatch <= kPend; i0 += 32 * kBatch) {
+      for (; i0 < we && np + 32 * kBatch <= pend_cap; i0 += 32 * kBatch) {
         int u[kBatch], c[kBatch];
 #pragma unroll
         for (int k = 0; k < kBatch; k++) {
@@ -833,7 +836,7 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
   for (int r = gc_core_size(ctl, core_cap) + gwarp; r < nbig; r += nwarps) {
     const int wv = __ldg(&order[r]);
     const int wb = __ldg(&nindex[wv]);
-    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, long_nap, status);
+    const int c = gc_long_row(wb, wb + __ldg(&hc[wv]), nl2, color, bits, pend, kPend, long_nap, status);
     if (c < 0) return;
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
@@ -896,10 +899,15 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   Carve c{ws};
   GCBufs b;
   gc_layout(c, g.n, g.m, &b);
+  // Blocks of the pull per SM: a knob, 2 by default.  Fewer warps poll
+  // fewer undecided entries at a time; on R-MAT-22 two blocks per SM colour
+  // faster than four (1.81 vs 2.15 ms) -- the polls of four blocks load L2
+  // enough to slow the dependency chain they wait on.
+  const int pull_blocks = dev.gc_pull_blocks > 0 ? dev.gc_pull_blocks : 2;
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
-  const int coop_grid = dev.sms * occ;
+  const int coop_grid = dev.sms * std::min(occ, pull_blocks);
   const int grid = dev.grid_blocks(kTPB);
   const RowChunks rc{b.chunks, &b.ctl->nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
   const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
@@ -932,9 +940,9 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
   ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
   mark();
-  // the long rows' polls back off to at most gc_poll_ns, 128 ns by default
+  // the long rows' polls back off to at most gc_poll_ns, 64 ns by default
   // (they carry the dependency chain; the short rows keep 512 ns)
-  const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 128u;
+  const unsigned long_nap = dev.gc_poll_ns > 0 ? (unsigned)dev.gc_poll_ns : 64u;
   ECL_CUDA_TRY(launch_cooperative(gc_pull, coop_grid, kTPB, stream, g.n, g.nindex, b.nl2, b.hc, order, color, b.ctl,
                                   cap, long_nap, status));
   mark();

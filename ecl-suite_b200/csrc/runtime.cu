@@ -23,7 +23,8 @@ bool tune_valid(const ecl_tune& t) {
   return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 8 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
          t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok &&
          (t.scc_sweep_batch == 0 || t.scc_sweep_batch == 1 || t.scc_sweep_batch == 2 || t.scc_sweep_batch == 4) &&
-         t.gc_poll_ns >= 0 && t.gc_poll_ns <= 4096 && (t.row_vec == 0 || t.row_vec == 1);
+         t.gc_poll_ns >= 0 && t.gc_poll_ns <= 4096 && (t.row_vec == 0 || t.row_vec == 1) &&
+         (t.gc_pull_blocks >= 0 && t.gc_pull_blocks <= 4);
 }
 
 void apply_tune(DeviceInfo* d, const ecl_tune& t) {
@@ -35,6 +36,7 @@ void apply_tune(DeviceInfo* d, const ecl_tune& t) {
   d->scc_sweep_batch = t.scc_sweep_batch;
   d->gc_poll_ns = t.gc_poll_ns;
   d->row_vec = t.row_vec;
+  d->gc_pull_blocks = t.gc_pull_blocks;
 }
 
 void set_last_error(const char* where, cudaError_t e) {

@@ -75,6 +75,7 @@ struct DeviceInfo {
   int scc_sweep_batch = 0;  // SCC: edges per lane in flight in a sweep (0 = default)
   int gc_poll_ns = 0;       // GC pull: longest back-off of a long row's polls, ns (0 = default)
   int row_vec = 0;          // CSR scans: 1 = warp rows read in 16-byte quads where aligned
+  int gc_pull_blocks = 0;   // GC pull: blocks per SM, 1..4 (0 = 2)
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }

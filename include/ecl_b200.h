@@ -94,9 +94,10 @@ typedef struct ecl_tune {
   int32_t row_chunk;      /* CSR scans: rows longer than this are cut into chunks of this many entries;
                              0 = per code, else a power of two in 128..8192 */
   int32_t scc_sweep_batch; /* SCC: edges per lane whose loads a sweep keeps in flight: 1, 2 or 4; 0 = 1 */
-  int32_t gc_poll_ns;      /* GC: longest sleep between polls of a long row's dependency, 0..4096 ns; 0 = 128 */
+  int32_t gc_poll_ns;      /* GC: longest sleep between polls of a long row's dependency, 0..4096 ns; 0 = 64 */
   int32_t row_vec;         /* CSR scans: 1 = warp rows read in 16-byte quads where aligned; 0 = 4-byte loads
                               (measured faster: the quads scatter the per-entry writes that follow) */
+  int32_t gc_pull_blocks;  /* GC pull: blocks of 256 threads per SM, 1..4; 0 = 2 */
 } ecl_tune;
 
 /* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);

@@ -277,8 +277,8 @@ def test_cc_validate_checks_the_symmetric_flag(ecl):
 
 @pytest.mark.parametrize("knobs", [dict(row_lane_max=1, row_chunk=128), dict(row_lane_max=8, row_chunk=512),
                                    dict(row_lane_max=32, row_chunk=8192, blocks_per_sm=2),
-                                   dict(mst_light_factor=0.4, gc_core_ranks=5),
-                                   dict(gc_poll_ns=2048, row_vec=1, scc_sweep_batch=4)])
+                                   dict(mst_light_factor=0.4, gc_core_ranks=5, gc_pull_blocks=4),
+                                   dict(gc_poll_ns=2048, row_vec=1, scc_sweep_batch=4, gc_pull_blocks=1)])
 def test_launch_knobs_never_change_results(ecl, orc, knobs):
     """Every code under non-default degree bins, grid sizes, MST split and GC
     core size gives the oracle's result (hub rows cross every chunk size)."""
