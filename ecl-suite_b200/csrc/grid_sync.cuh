@@ -36,7 +36,9 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, Status* status) {
           ok = 0;
           break;
         }
-        if (ld(&status->code) != 0) {
+        // an error anywhere ends the wait; read every 64th spin, as every
+        // waiting block polling one more word would crowd its L2 slice
+        if ((spins & 63u) == 0 && ld(&status->code) != 0) {
           ok = 0;
           break;
         }
