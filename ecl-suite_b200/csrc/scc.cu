@@ -28,8 +28,11 @@
 //    atomic max on one half.  Trimmed vertices hold a DEAD word that every
 //    sweep skips.  Each lane keeps kSweepBatch edges' loads in flight (a
 //    launch knob: 1, 2 or 4; fewer edges a lane leave more lanes resident);
-//  * rounds after the first compact the surviving edges (the edges whose two
-//    ends share both values and are unresolved: io[v] == io[w]);
+//  * rounds after the first sweep only the surviving edges (the edges whose
+//    two ends share both values and are unresolved: io[v] == io[w]); every
+//    sweep appends the edges it would keep, and the round's last sweep --
+//    which raised nothing, so it read final words -- leaves the next round's
+//    list without a separate pass;
 //  * the final labels are written by the same launch (label = in-max).
 #include "csr_bins.cuh"
 #include "grid_sync.cuh"
@@ -44,16 +47,27 @@ constexpr int kTPB = 256;
 constexpr int kMaxSweeps = 1 << 16;
 constexpr int kScanBatch = 4;  // list entries per lane whose loads are issued together
 
+constexpr int kStamps = 256;
+
 struct SCCCtl {
   GridBarrier bar;
   int pad[64];
+  // %globaltimer at the start and after each grid barrier (the first
+  // kStamps - 1): a time profile of sweeps, compactions and retirements that
+  // costs one store per barrier
+  unsigned long long stamp[kStamps];
   int changed[kMaxSweeps];   // per-sweep "something moved" flags
+  int raised[kMaxSweeps];    // per-sweep counts of raises
+  int kept[kMaxSweeps];      // per-sweep sizes of the list of edges a round keeps
+  int again[kMaxSweeps];     // per-round "vertices left" flags, indexed by the round's last sweep
 };
 
-struct SCCRound {
-  int size;
-  int again;
-};
+__device__ __forceinline__ unsigned long long scc_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 
 // In-max (high half) and out-max (low half) of one vertex.
 __device__ __forceinline__ unsigned long long io_pack(int in, int out) {
@@ -187,15 +201,18 @@ template <int kSweepBatch>
 __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve(int n, int m0, int2* __restrict__ wlA, int2* __restrict__ wlB,
                                                   const int* __restrict__ flags, unsigned long long* __restrict__ io,
                                                   int* __restrict__ label, SCCCtl* __restrict__ ctl,
-                                                  SCCRound* __restrict__ rounds, int max_rounds,
+                                                  int max_rounds,
                                                   Status* __restrict__ status) {
   const int lane = threadIdx.x & 31;
   const int tid = blockIdx.x * kTPB + threadIdx.x;
   const int nthreads = gridDim.x * kTPB;
+  int nstamp = 0;  // thread 0: stamps written
+  if (tid == 0) ctl->stamp[0] = scc_now();
   // 0. live vertices start at (v, v); trimmed ones are DEAD
   for (int v = tid; v < n; v += nthreads)
     io[v] = __ldg(&flags[v]) == (kHasIn | kHasOut) ? io_pack(v, v) : kDead;  // race-free: owned, barrier next
   if (!grid_sync(&ctl->bar, status)) return;
+  if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
   int size = m0;
   int sweep = 0;
   int round = 0;
@@ -212,7 +229,13 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
         raise(status, ECL_ERR_NO_CONVERGENCE, -sweep);
         return;
       }
-      bool moved = false;
+      int raises = 0;
+      // Append the edges this round keeps during the sweep (below) once the
+      // last sweep raised few words: the values are then close to final, and
+      // few edges look kept.  Earlier, transient agreement makes millions of
+      // edges look kept, and their appends would cost more than the
+      // separate pass they save.
+      const bool spec = sweep > 0 && ld(&ctl->raised[sweep - 1]) <= (m0 >> 6);
       // The jump targets converge on a few vertices (the largest SCC's
       // maximum id first of all), so every thread keeps its last jump of
       // each kind: a repeated target reuses the value instead of loading the
@@ -266,36 +289,63 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
             }
             if (ow[k] == c_ow) ow[k] = max(ow[k], c_out);
           }
-          if (iv[k] >= 0 && io_raise<true>(&io[e[k].y], B[k], iv[k])) moved = true;
+          if (iv[k] >= 0 && io_raise<true>(&io[e[k].y], B[k], iv[k])) raises++;
           const int v = iv[k] >= 0 ? e[k].x : -1;
           const unsigned grp = __match_any_sync(kFull, v);
           const int gow = __reduce_max_sync(grp, ow[k]);
-          if (v >= 0 && lane == __ffs(grp) - 1 && io_raise<false>(&io[v], A[k], gow)) moved = true;
+          if (v >= 0 && lane == __ffs(grp) - 1 && io_raise<false>(&io[v], A[k], gow)) raises++;
+        }
+        // The edges the round keeps (endpoints unresolved and in full
+        // agreement), judged by the words this sweep loaded: only the last
+        // sweep's list is used, and that sweep raised nothing, so its words
+        // were final.  This saves a separate pass over the list and its words.
+        if (spec) {
+#pragma unroll
+          for (int k = 0; k < kSweepBatch; k++) {
+            const bool keep = A[k] != kDead && io_in(A[k]) != io_out(A[k]) && A[k] == B[k];
+            const int at = warp_append(&ctl->kept[sweep], keep);
+            if (keep && at < m0) nxt[at] = e[k];
+          }
         }
       }
-      if (__any_sync(kFull, moved) && lane == 0) st(&ctl->changed[sweep], 1);
+      // one count per block (a flag per warp would queue at one word)
+      __shared__ int s_raises;
+      if (threadIdx.x == 0) s_raises = 0;
+      __syncthreads();
+      const int wr = __reduce_add_sync(kFull, raises);
+      if (lane == 0 && wr) atomicAdd(&s_raises, wr);  // shared memory
+      __syncthreads();
+      if (threadIdx.x == 0 && s_raises) {
+        fetch_add(&ctl->raised[sweep], s_raises);
+        st(&ctl->changed[sweep], 1);
+      }
       if (!grid_sync(&ctl->bar, status)) return;
+  if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
       const bool again = ld(&ctl->changed[sweep]) != 0;
       sweep++;
-      if (!again) break;
-    }
-    // 2. keep the edges whose endpoints are unresolved and agree
-    for (int i0 = tid - lane; i0 < size; i0 += nthreads) {
-      const int i = i0 + lane;
-      bool keep = false;
-      int2 e = make_int2(0, 0);
-      if (i < size) {
-        e = cur[i];
-        if ((unsigned)e.x < (unsigned)n && (unsigned)e.y < (unsigned)n) {
-          const unsigned long long A = ld(&io[e.x]);
-          keep = A != kDead && io_in(A) != io_out(A) && A == ld(&io[e.y]);
+      if (!again) {
+        if (spec) break;
+        // 1b. the last sweep kept no list: keep the edges whose endpoints are
+        // unresolved and agree, in a pass of its own
+        for (int i0 = tid - lane; i0 < size; i0 += nthreads) {
+          const int i = i0 + lane;
+          bool keep = false;
+          int2 e = make_int2(0, 0);
+          if (i < size) {
+            e = cur[i];
+            if ((unsigned)e.x < (unsigned)n && (unsigned)e.y < (unsigned)n) {
+              const unsigned long long A = ld(&io[e.x]);
+              keep = A != kDead && io_in(A) != io_out(A) && A == ld(&io[e.y]);
+            }
+          }
+          const int at = warp_append(&ctl->kept[sweep - 1], keep);
+          if (keep && at < m0) nxt[at] = e;
         }
+        if (!grid_sync(&ctl->bar, status)) return;
+        break;
       }
-      const int at = warp_append(&rounds[round].size, keep);
-      if (keep) nxt[at] = e;
     }
-    if (!grid_sync(&ctl->bar, status)) return;
-    // 3. retire resolved (and trimmed) vertices, reset the rest to their own id
+    // 2. retire resolved (and trimmed) vertices, reset the rest to their own id
     bool again = false;
     for (int v = tid; v < n; v += nthreads) {
       const unsigned long long A = ld(&io[v]);
@@ -308,10 +358,11 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
         again = true;
       }
     }
-    if (__any_sync(kFull, again) && lane == 0) st(&rounds[round].again, 1);
+    if (__any_sync(kFull, again) && lane == 0) st(&ctl->again[sweep - 1], 1);
     if (!grid_sync(&ctl->bar, status)) return;
-    if (!ld(&rounds[round].again)) break;
-    size = ld(&rounds[round].size);
+  if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
+    if (!ld(&ctl->again[sweep - 1])) break;
+    size = min(ld(&ctl->kept[sweep - 1]), m0);
     int2* t = cur;
     cur = nxt;
     nxt = t;
@@ -321,7 +372,6 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
 
 struct SCCBufs {
   SCCCtl* ctl;
-  SCCRound* rounds;
   int* flags;
   int* nchunks;
   int2* chunks;
@@ -334,7 +384,6 @@ struct SCCBufs {
 void scc_layout(Carve& c, int n, int m, SCCBufs* b) {
   b->ctl = c.take<SCCCtl>(1);
   b->max_rounds = n + 1;
-  b->rounds = c.take<SCCRound>((size_t)b->max_rounds);
   b->flags = c.take<int>((size_t)n);
   b->nchunks = c.take<int>(64);
   b->chunks = c.take<int2>(row_chunk_capacity(m, kMinChunk));
@@ -362,7 +411,7 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   SCCBufs b;
   scc_layout(c, g.n, g.m, &b);
   const int batch = dev.scc_sweep_batch > 0 ? dev.scc_sweep_batch : kSweepBatchDefault;
-  void (*solve)(int, int, int2*, int2*, const int*, unsigned long long*, int*, SCCCtl*, SCCRound*, int, Status*) =
+  void (*solve)(int, int, int2*, int2*, const int*, unsigned long long*, int*, SCCCtl*, int, Status*) =
       batch == 1 ? scc_solve<1> : (batch == 4 ? scc_solve<4> : scc_solve<2>);
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve, kTPB, 0) != cudaSuccess || occ < 1)
@@ -372,8 +421,6 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (max_rounds <= 0 || max_rounds > b.max_rounds) max_rounds = b.max_rounds;
 
   if (cudaMemsetAsync(b.ctl, 0, sizeof(SCCCtl), stream) != cudaSuccess) return ECL_ERR_CUDA;
-  if (cudaMemsetAsync(b.rounds, 0, sizeof(SCCRound) * (size_t)b.max_rounds, stream) != cudaSuccess)
-    return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.flags, 0, sizeof(int) * (size_t)g.n, stream) != cudaSuccess) return ECL_ERR_CUDA;
   if (cudaMemsetAsync(b.nchunks, 0, sizeof(int), stream) != cudaSuccess) return ECL_ERR_CUDA;
   const RowChunks rc{b.chunks, b.nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
@@ -384,7 +431,7 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
              status);
   mark();
   ECL_CUDA_TRY(launch_cooperative(solve, coop_grid, kTPB, stream, g.n, g.m, b.wlA, b.wlB, b.flags, b.io, label, b.ctl,
-                                  b.rounds, max_rounds, status));
+                                  max_rounds, status));
   mark();
   return ECL_OK;
 }
