@@ -549,10 +549,15 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     // per-thread memos: roots cannot change during phase A (joins happen in
     // phase B), so a remembered find is exact
     MstMemo fx, fy, px, py;
+    // each step's entry is loaded one step ahead (the stream's latency then
+    // overlaps the previous step's finds and publishes)
+    int4 nx = tid < sz ? __ldcs(&in[tid]) : make_int4(-1, -1, 0, 0);
     for (int it = 0; it < iters; it++) {
       const int i = tid + it * nthreads;
       const bool valid = i < sz;
-      const int4 e = valid ? __ldcs(&in[i]) : make_int4(-1, -1, 0, 0);
+      const int4 e = nx;
+      const long long i1 = (long long)i + nthreads;
+      nx = i1 < sz ? __ldcs(&in[i1]) : make_int4(-1, -1, 0, 0);
       // one find per distinct endpoint per warp (the lanes holding it share
       // the result)
       const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
@@ -600,10 +605,13 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
     }
     __syncthreads();
     MstMemo kxm, kym;
+    int4 nxb = tid < nsz ? __ldcs(&out[tid]) : make_int4(-1, -1, 0, 0);  // one step ahead, as in phase A
     for (int i0 = tid - lane; i0 < nsz; i0 += nthreads) {
       const int i = i0 + lane;
       const bool valid = i < nsz;
-      const int4 e = valid ? __ldcs(&out[i]) : make_int4(-1, -1, 0, 0);
+      const int4 e = nxb;
+      const long long i1 = (long long)i + nthreads;
+      nxb = i1 < nsz ? __ldcs(&out[i1]) : make_int4(-1, -1, 0, 0);
       const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
       const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
       u64 kx = 0, ky = 0;

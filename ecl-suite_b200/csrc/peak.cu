@@ -99,6 +99,103 @@ extern "C" ecl_status ecl_minplus_peak(int32_t variant, double* ops_per_s) {
   return ECL_OK;
 }
 
+// ---- streaming gather rate ------------------------------------------------------
+//
+// The roofline of the CSR scans: every scan streams the 4-byte column indices
+// once and, per entry, loads one word of a per-vertex array that stays in L2
+// (GC's keys, MST's roots, SCC's flags).  This probe does exactly that and
+// nothing else -- each index (read once, coalesced, evict-first) selects one
+// 8-byte word of an n-word table, kGatherBatch entries in flight per lane --
+// so the rate it reaches on a graph's own index array bounds any scan of that
+// graph.  Variant 0 loads the words through the read-only path (__ldg, as
+// GC's keys are read), variant 1 with relaxed device-scope atomic loads (as
+// MST's roots and SCC's flags are).
+namespace ecl {
+namespace {
+
+constexpr int kGatherBatch = 4;
+
+template <bool kCoherent>
+__global__ void __launch_bounds__(kPeakThreads) gather_kernel(const int* __restrict__ idx, int m,
+                                                             const unsigned long long* __restrict__ table, int n,
+                                                             unsigned long long* __restrict__ sink) {
+  const int tid = blockIdx.x * kPeakThreads + threadIdx.x;
+  const int nthreads = gridDim.x * kPeakThreads;
+  unsigned long long acc = 0;
+  for (long long j0 = tid; j0 < m; j0 += (long long)nthreads * kGatherBatch) {
+    int u[kGatherBatch];
+#pragma unroll
+    for (int k = 0; k < kGatherBatch; k++) {
+      const long long j = j0 + (long long)k * nthreads;
+      u[k] = j < m ? __ldcs(&idx[j]) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < kGatherBatch; k++)
+      if ((unsigned)u[k] < (unsigned)n) acc += kCoherent ? dev::ld(&table[u[k]]) : __ldg(&table[u[k]]);
+  }
+  sink[tid] = acc;  // thread-owned: keeps every load live
+}
+
+}  // namespace
+}  // namespace ecl
+
+extern "C" ecl_status ecl_gather_peak(const int32_t* d_index, int32_t m, int32_t n, int32_t variant,
+                                      double* entries_per_s) {
+  using namespace ecl;
+  if (!entries_per_s || !d_index || m <= 0 || n <= 0 || (variant != 0 && variant != 1)) {
+    set_last_error_msg("ecl_gather_peak: need a device index array, m > 0, n > 0, variant 0 or 1");
+    return ECL_ERR_INVALID_ARG;
+  }
+  *entries_per_s = 0.0;
+  DeviceInfo di;
+  const ecl_status st = current_device(&di);
+  if (st != ECL_OK) return st;
+  int per_sm = 0;
+  ECL_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, variant == 0 ? gather_kernel<false> : gather_kernel<true>, kPeakThreads, 0));
+  const int blocks = di.sms * (per_sm > 0 ? per_sm : 1);
+  unsigned long long* table = nullptr;
+  unsigned long long* sink = nullptr;
+  char* flush = nullptr;
+  const size_t flush_bytes = 256ull << 20;  // more than the 126 MB L2: every timed run starts cold
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t err = cudaMalloc(&table, sizeof(unsigned long long) * (size_t)n);
+  if (err == cudaSuccess) err = cudaMalloc(&sink, sizeof(unsigned long long) * (size_t)blocks * kPeakThreads);
+  if (err == cudaSuccess) err = cudaMalloc(&flush, flush_bytes);
+  if (err == cudaSuccess) err = cudaMemset(table, 0x5a, sizeof(unsigned long long) * (size_t)n);
+  if (err == cudaSuccess) err = cudaEventCreate(&e0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e1);
+  float best_ms = 0.0f;
+  for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {  // rep 0 warms up
+    // cold L2 for the index stream, then the table alone warmed into L2, as
+    // a scan finds its per-vertex array after the kernels before it
+    err = cudaMemsetAsync(flush, rep, flush_bytes, 0);
+    if (err == cudaSuccess) err = cudaMemsetAsync(table, 0x5a, sizeof(unsigned long long) * (size_t)n, 0);
+    if (err != cudaSuccess) break;
+    cudaEventRecord(e0, 0);
+    if (variant == 0)
+      ECL_LAUNCH(gather_kernel<false>, blocks, kPeakThreads, 0, 0, d_index, m, table, n, sink);
+    else
+      ECL_LAUNCH(gather_kernel<true>, blocks, kPeakThreads, 0, 0, d_index, m, table, n, sink);
+    cudaEventRecord(e1, 0);
+    err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(table);
+  cudaFree(sink);
+  cudaFree(flush);
+  if (err != cudaSuccess || best_ms <= 0.0f) {
+    set_last_error("ecl_gather_peak", err);
+    return ECL_ERR_CUDA;
+  }
+  *entries_per_s = (double)m / (best_ms * 1e-3);
+  return ECL_OK;
+}
+
 // ---- dependency-hop latency ----------------------------------------------------
 //
 // One hop of a dependency chain: a warp stores a value another warp is

@@ -102,6 +102,7 @@ _sig("ecl_workspace_bytes", C.c_size_t, [C.c_int, _I32, _I32])
 _sig("ecl_kernel_launches", C.c_uint64, [])
 _sig("ecl_minplus_peak", C.c_int, [C.c_int32, C.POINTER(C.c_double)])
 _sig("ecl_hop_latency", C.c_int, [C.c_int32, C.POINTER(C.c_double)])
+_sig("ecl_gather_peak", C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)])
 _sig("ecl_gc_critical_path", C.c_int, [_PV, C.c_int32, C.c_double, C.c_double, C.POINTER(C.c_int32),
                                         C.POINTER(C.c_int32), C.POINTER(C.c_double)])
 _sig("ecl_cc", C.c_int, [_PV, _VP, _PO])
@@ -121,7 +122,7 @@ _sig("ecl_gen_er", C.c_int, [_I32, _F64, _U64, _I32, _U64, _I32, _I32, _PG])
 # Every symbol that include/ecl_b200.h declares (checked by the CPU tests).
 EXPORTED = [
     "ecl_abi_version", "ecl_status_string", "ecl_last_error", "ecl_workspace_bytes", "ecl_kernel_launches",
-    "ecl_minplus_peak", "ecl_hop_latency", "ecl_gc_critical_path", "ecl_set_tune", "ecl_get_tune",
+    "ecl_minplus_peak", "ecl_hop_latency", "ecl_gather_peak", "ecl_gc_critical_path", "ecl_set_tune", "ecl_get_tune",
     "ecl_cc", "ecl_mis", "ecl_gc", "ecl_mst", "ecl_scc", "ecl_apsp",
     "ecl_compute_cc", "ecl_compute_mis", "ecl_compute_gc", "ecl_compute_mst", "ecl_compute_scc", "ecl_compute_apsp",
     "ecl_graph_read", "ecl_graph_write", "ecl_graph_free", "ecl_graph_validate",
@@ -384,6 +385,16 @@ def hop_latency(variant: int = 0) -> float:
     1: L2 with a bare spin, 2: shared memory between two warps of a CTA)."""
     v = C.c_double(0.0)
     _check(lib.ecl_hop_latency(variant, C.byref(v)), "ecl_hop_latency")
+    return float(v.value)
+
+
+def gather_peak(index, n: int, variant: int = 0) -> float:
+    """Measured streaming-gather rate, entries/s: each of the device indices
+    `index` (a CUDA int32 tensor, values in [0, n)) loads one 8-byte word of
+    an L2-resident n-word table (0: read-only loads, 1: relaxed atomic loads)
+    -- the roofline of a CSR scan over a graph with those column indices."""
+    v = C.c_double(0.0)
+    _check(lib.ecl_gather_peak(_ptr(index), int(index.numel()), n, variant, C.byref(v)), "ecl_gather_peak")
     return float(v.value)
 
 

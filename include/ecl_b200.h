@@ -139,6 +139,14 @@ ecl_status ecl_minplus_peak(int32_t variant, double* ops_per_s);
  * of one CTA through shared memory, polled the way GC's core polls.  The
  * latency denominators of GC's roofline.  No counterpart in the reference. */
 ecl_status ecl_hop_latency(int32_t variant, double* ns_per_hop);
+/* Measured streaming-gather rate of the current device, in entries per second:
+ * the m device indices d_index[0..m) (each in [0, n)) are read once and each
+ * loads one 8-byte word of an n-word table that sits in L2 -- the work per
+ * entry of every CSR scan here (GC's key, MST's root, SCC's flag), and so the
+ * roofline of a scan over a graph whose column indices are d_index.  variant 0
+ * loads through the read-only path, 1 with relaxed device-scope atomic loads.
+ * No counterpart in the reference. */
+ecl_status ecl_gather_peak(const int32_t* d_index, int32_t m, int32_t n, int32_t variant, double* entries_per_s);
 /* GC's critical path, computed on the host for a host graph: *hops = the
  * longest chain of higher-priority dependencies (ECL-GC-atomic.cu:102
  * priorities), *hops_core = its part inside the first min(long rows,
