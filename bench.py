@@ -638,7 +638,7 @@ def bench_plain(args, rank, world, local_rank):
     scan_roof = None
     if args.workload == "suite":
         scans = [(("gc", 0), "read-only"), (("mst", 1), "read-only"), (("mst", 3), "atomic"),
-                 (("scc", 0), "atomic"), (("mis", 1), "atomic")]
+                 (("scc", 0), "atomic")]
         graph_of = {phase_code(c, gg): gg for c, gg in jobs}
         peak_cache = {}
         scan_roof = {}

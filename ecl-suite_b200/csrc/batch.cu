@@ -430,7 +430,8 @@ ecl_status ecl_batch_tune(ecl_batch* b, int32_t trials, ecl_tune* best) {
       {(b->codes & ECL_BATCH_MST) != 0, {0.75f, 1.5f, 3.f, 0.4f}, [](ecl_tune& t, float v) { t.mst_light_factor = v; }},
       {true, {32.f, 16.f, 8.f}, [](ecl_tune& t, float v) { t.row_lane_max = (int32_t)v; }},
       {true, {256.f, 128.f, 512.f, 2048.f}, [](ecl_tune& t, float v) { t.row_chunk = (int32_t)v; }},
-      {(b->codes & ECL_BATCH_GC) != 0, {4096.f, 16384.f, 1024.f}, [](ecl_tune& t, float v) { t.gc_core_ranks = (int32_t)v; }},
+      {(b->codes & ECL_BATCH_GC) != 0, {8192.f, 4096.f, 16384.f}, [](ecl_tune& t, float v) { t.gc_core_ranks = (int32_t)v; }},
+      {(b->codes & ECL_BATCH_GC) != 0, {2.f, 1.f, 4.f}, [](ecl_tune& t, float v) { t.gc_core_ctas = (int32_t)v; }},
       {(b->codes & ECL_BATCH_GC) != 0, {2.f, 4.f, 1.f}, [](ecl_tune& t, float v) { t.gc_pull_blocks = (int32_t)v; }},
       {(b->codes & ECL_BATCH_SCC) != 0, {1.f, 2.f, 4.f}, [](ecl_tune& t, float v) { t.scc_sweep_batch = (int32_t)v; }},
   };

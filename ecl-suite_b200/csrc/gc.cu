@@ -429,8 +429,13 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
 // row's length, below 2^15).
 constexpr int kCoreThreads = 1024;
 constexpr int kCoreWarps = kCoreThreads / 32;
+// Default CTAs of the core's cluster.  R-MAT-22, core + pull: 1 CTA with 4096
+// ranks 3.15 ms; 2 CTAs with 8192 ranks 2.86 ms; 4 CTAs 2.92 ms (a hop
+// between CTAs, through distributed shared memory, costs more than one inside
+// a CTA, so more CTAs than two buy nothing).
+constexpr int kCoreCtas = 2;
 constexpr int kCoreBatch = 4;           // entries per lane whose loads are in flight together
-constexpr int kCoreDefault = 4096;      // default core size (ranks): the measured best at R-MAT-22
+constexpr int kCoreDefault = 8192;      // default core size (ranks): the measured best at R-MAT-22 with 2 CTAs
 constexpr int kCoreMax = 36864;         // shared memory bound
 constexpr int kSegSlack = 8;            // a buffer holds a segment plus its 16-byte alignment slack
 constexpr int kCorePend = 1024;         // per-warp list of undecided entries (16-bit ranks)
@@ -493,13 +498,42 @@ __global__ void __launch_bounds__(kTPB) gc_core_translate(const int* __restrict_
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 // 16-bit colour words: relaxed CTA-scope atomic loads and stores.
+// The core's colours live in every CTA of its cluster (one copy per CTA's
+// shared memory): a colour is stored into each copy (distributed shared
+// memory) and read from the local one, so both sides are cluster-scope
+// relaxed accesses.
 __device__ __forceinline__ unsigned col_ld(const unsigned short* p) {
   unsigned short v;
-  asm volatile("ld.relaxed.cta.shared.u16 %0, [%1];" : "=h"(v) : "r"(smem_u32(p)) : "memory");
+  asm volatile("ld.relaxed.cluster.shared::cta.u16 %0, [%1];" : "=h"(v) : "r"(smem_u32(p)) : "memory");
   return v;
 }
 __device__ __forceinline__ void col_st(unsigned short* p, unsigned v) {
-  asm volatile("st.relaxed.cta.shared.u16 [%0], %1;" ::"r"(smem_u32(p)), "h"((unsigned short)v) : "memory");
+  asm volatile("st.relaxed.cluster.shared::cta.u16 [%0], %1;" ::"r"(smem_u32(p)), "h"((unsigned short)v) : "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_ctas() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// Every thread of every CTA of the cluster; memory before it is visible to
+// the whole cluster after it.
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+// Stores colour v of the rank at p (a local shared address) into the copy of
+// every CTA of the cluster.
+__device__ __forceinline__ void col_publish(unsigned short* p, unsigned v, int ctas) {
+  const unsigned local = smem_u32(p);
+  for (int k = 0; k < ctas; k++) {
+    unsigned remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local), "r"(k));
+    asm volatile("st.relaxed.cluster.shared::cluster.u16 [%0], %1;" ::"r"(remote), "h"((unsigned short)v) : "memory");
+  }
 }
 
 __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
@@ -661,13 +695,19 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
                                                            int cap, Status* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char s_core[];
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1;
   const int core = gc_core_size(ctl, cap);
+  // The core runs on a cluster of `ctas` CTAs (1 without a cluster launch):
+  // rank r belongs to warp r mod (32 ctas) of the cluster, so each CTA takes
+  // every ctas-th block of 32 consecutive ranks (dealing longer runs of
+  // consecutive ranks to one CTA measured slower; single ranks, no faster).
+  const int ctas = (int)cluster_ctas();
+  const int warp = (int)cluster_rank() * kCoreWarps + (threadIdx.x >> 5);
+  const int cwarps = ctas * kCoreWarps;
   unsigned short* col_s = reinterpret_cast<unsigned short*>(s_core);
   const int segbuf = gc_core_segbuf(cap);
   const int kSeg = segbuf - kSegSlack;  // row entries staged at a time
-  unsigned char* wbase = s_core + gc_core_colour_bytes(cap) + (size_t)warp * gc_core_warp_bytes(segbuf);
+  unsigned char* wbase = s_core + gc_core_colour_bytes(cap) + (size_t)(threadIdx.x >> 5) * gc_core_warp_bytes(segbuf);
   CoreStage stg;
   stg.bar[0] = reinterpret_cast<unsigned long long*>(wbase);
   stg.bar[1] = stg.bar[0] + 1;
@@ -682,25 +722,26 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
     mbar_fence_init();
   }
   __syncthreads();
+  if (ctas > 1) cluster_sync();  // every copy is initialised before any colour is stored into it
 
-  // Row j of this warp is rank warp + 32 j; lane L holds the row record of
-  // row jb + L (records are fetched 32 rows at a time).
+  // Row j of this warp is rank warp + cwarps j; lane L holds the row record
+  // of row jb + L (records are fetched 32 rows at a time).
   int jb = -32;
   int4 rec = make_int4(0, 0, -1, 0);
   auto row_of = [&](int j) -> int4 {  // all lanes call
     if ((j & ~31) != jb) {
       jb = j & ~31;
-      const int r = warp + 32 * (jb + lane);
+      const int r = warp + cwarps * (jb + lane);
       rec = r < core ? __ldg(&rowinfo[r]) : make_int4(0, 0, -1, 0);
     }
     const int src = j & 31;
     return make_int4(__shfl_sync(kFull, rec.x, src), __shfl_sync(kFull, rec.y, src), __shfl_sync(kFull, rec.z, src),
                      0);
   };
-  const int nrows = core > warp ? (core - warp + kCoreWarps - 1) / kCoreWarps : 0;
+  const int nrows = core > warp ? (core - warp + cwarps - 1) / cwarps : 0;
   int b = 0;  // buffer holding (or about to hold) the segment to scan next
   for (int j = 0; j < nrows; j++) {
-    const int r = warp + kCoreWarps * j;
+    const int r = warp + cwarps * j;
     const int4 row = row_of(j);
     const int wb = row.x, h = row.y, v = row.z;
     bits[lane] = 0;
@@ -781,7 +822,7 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
     }
     if (stalled) {
       stg.drain();
-      return;
+      break;
     }
     // the smallest colour of the first window the bitmap leaves free
     __syncwarp();
@@ -800,15 +841,18 @@ __global__ void __launch_bounds__(kCoreThreads, 1) gc_core(const int* __restrict
       c = gc_core_row_global(r, wb, wb + h, 32 * kMexWords, nl2, col_s, bits, pend, status);
       if (c < 0) {
         stg.drain();
-        return;
+        break;
       }
     }
     if (lane == 0) {
-      col_st(&col_s[r], (unsigned)c);
+      col_publish(&col_s[r], (unsigned)c, ctas);
       st(&color[v], c);
     }
     __syncwarp();
   }
+  // a CTA's shared memory must outlive every store the others make into it:
+  // every warp, done or given up (each wait is bounded), meets here
+  if (ctas > 1) cluster_sync();
 }
 
 __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ nindex, const int* __restrict__ nl2,
@@ -937,7 +981,33 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   ECL_LAUNCH(gc_core_rank, grid, kTPB, 0, stream, order, rank, b.ctl, cap);
   ECL_LAUNCH(gc_core_translate, grid, kTPB, 0, stream, g.nindex, b.nl2, b.hc, order, rank, b.rowinfo, b.ctl, cap);
   ECL_CUDA_TRY(cudaFuncSetAttribute(gc_core, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gc_core_smem(cap)));
-  ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
+  // the core's cluster: as many CTAs as asked for when such a cluster fits
+  // the device, else one CTA
+  const int want = dev.gc_core_ctas > 0 ? dev.gc_core_ctas : kCoreCtas;
+  int ctas = 1;
+  if (want > 1) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)want);
+    cfg.blockDim = dim3((unsigned)kCoreThreads);
+    cfg.dynamicSmemBytes = gc_core_smem(cap);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)want;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, gc_core, &cfg) == cudaSuccess && clusters >= 1)
+      ctas = want;
+    else
+      cudaGetLastError();  // no such cluster here: one CTA
+  }
+  if (ctas > 1)
+    ECL_CUDA_TRY(launch_cluster(gc_core, ctas, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color,
+                                b.ctl, cap, status));
+  else
+    ECL_LAUNCH(gc_core, 1, kCoreThreads, gc_core_smem(cap), stream, b.nl2, b.rowinfo, color, b.ctl, cap, status);
   mark();
   // the long rows' polls back off to at most gc_poll_ns, 64 ns by default
   // (they carry the dependency chain; the short rows keep 512 ns)

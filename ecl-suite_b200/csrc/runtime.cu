@@ -24,7 +24,7 @@ bool tune_valid(const ecl_tune& t) {
          t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok &&
          (t.scc_sweep_batch == 0 || t.scc_sweep_batch == 1 || t.scc_sweep_batch == 2 || t.scc_sweep_batch == 4) &&
          t.gc_poll_ns >= 0 && t.gc_poll_ns <= 4096 && (t.row_vec == 0 || t.row_vec == 1) &&
-         (t.gc_pull_blocks >= 0 && t.gc_pull_blocks <= 4);
+         (t.gc_pull_blocks >= 0 && t.gc_pull_blocks <= 4) && t.gc_core_ctas >= 0 && t.gc_core_ctas <= 8;
 }
 
 void apply_tune(DeviceInfo* d, const ecl_tune& t) {
@@ -37,6 +37,7 @@ void apply_tune(DeviceInfo* d, const ecl_tune& t) {
   d->gc_poll_ns = t.gc_poll_ns;
   d->row_vec = t.row_vec;
   d->gc_pull_blocks = t.gc_pull_blocks;
+  d->gc_core_ctas = t.gc_core_ctas;
 }
 
 void set_last_error(const char* where, cudaError_t e) {

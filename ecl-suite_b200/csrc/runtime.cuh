@@ -40,6 +40,28 @@ void set_last_error_msg(const char* msg);
     ::ecl::count_launch();                                        \
   } while (0)
 
+// One thread-block cluster of `ctas` CTAs (its CTAs share distributed shared
+// memory), through cudaLaunchKernelEx and the cluster-dimension attribute.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_cluster(void (*kernel)(KArgs...), int ctas, int block, size_t smem, cudaStream_t stream,
+                           Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ctas);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)ctas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+  count_launch();
+  return e;
+}
+
 // Cooperative (all blocks co-resident) launch through cudaLaunchKernelEx and
 // the cooperative launch attribute, which stream capture turns into a
 // cooperative CUDA-graph kernel node.
@@ -76,6 +98,7 @@ struct DeviceInfo {
   int gc_poll_ns = 0;       // GC pull: longest back-off of a long row's polls, ns (0 = default)
   int row_vec = 0;          // CSR scans: 1 = warp rows read in 16-byte quads where aligned
   int gc_pull_blocks = 0;   // GC pull: blocks per SM, 1..4 (0 = 2)
+  int gc_core_ctas = 0;     // GC core: CTAs of its cluster, 1..8 (0 = 2)
   // Grid of a grid-stride kernel with `tpb` threads per block: by default
   // every SM filled to its thread limit.
   int grid_blocks(int tpb) const { return sms * (blocks_per_sm > 0 ? blocks_per_sm : max_threads_per_sm / tpb); }

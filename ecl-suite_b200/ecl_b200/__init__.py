@@ -419,7 +419,7 @@ class Tune(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_int32), ("mst_light_factor", C.c_float), ("gc_core_ranks", C.c_int32),
                 ("row_lane_max", C.c_int32), ("row_chunk", C.c_int32), ("scc_sweep_batch", C.c_int32),
                 ("gc_poll_ns", C.c_int32), ("row_vec", C.c_int32),
-                ("gc_pull_blocks", C.c_int32)]
+                ("gc_pull_blocks", C.c_int32), ("gc_core_ctas", C.c_int32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

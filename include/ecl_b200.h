@@ -89,7 +89,7 @@ typedef struct ecl_opts {
 typedef struct ecl_tune {
   int32_t blocks_per_sm;  /* blocks of 256 threads per SM for the grid-stride kernels; 0 = fill the SM */
   float mst_light_factor; /* MST light-edge target, in multiples of n; 0 = 0.75 */
-  int32_t gc_core_ranks;  /* GC: leading ranks coloured in one CTA's shared memory, 0..36864; 0 = 4096 */
+  int32_t gc_core_ranks;  /* GC: leading ranks coloured in shared memory (the core), 0..36864; 0 = 8192 */
   int32_t row_lane_max;   /* CSR scans: rows of at most this many entries go to one lane, 0..32; 0 = per code */
   int32_t row_chunk;      /* CSR scans: rows longer than this are cut into chunks of this many entries;
                              0 = per code, else a power of two in 128..8192 */
@@ -98,6 +98,7 @@ typedef struct ecl_tune {
   int32_t row_vec;         /* CSR scans: 1 = warp rows read in 16-byte quads where aligned; 0 = 4-byte loads
                               (measured faster: the quads scatter the per-entry writes that follow) */
   int32_t gc_pull_blocks;  /* GC pull: blocks of 256 threads per SM, 1..4; 0 = 2 */
+  int32_t gc_core_ctas;    /* GC core: CTAs of the cluster that colours it, 1..8; 0 = 2 */
 } ecl_tune;
 
 /* Process-wide knobs of the single-graph entry points (ecl_cc ... ecl_scc);

@@ -86,19 +86,22 @@ def test_gc_large_colour_windows(ecl, orc):
 
 
 @pytest.mark.parametrize("core", [1, 7, 64, 0])
-def test_gc_core_size_does_not_change_colours(ecl, orc, core):
-    """The leading ranks are coloured in one CTA's shared memory and the rest
-    by the grid-wide pull; where the boundary lies (1, 7, 64 ranks, or the
-    default of 4096) changes no colour.  A 2100-clique (every vertex a long
-    row inside the default core) forces colours past the first 2048-colour
-    window there."""
-    old = ecl.set_tune(gc_core_ranks=core)
+@pytest.mark.parametrize("ctas", [0, 1, 4])
+def test_gc_core_size_does_not_change_colours(ecl, orc, core, ctas):
+    """The leading ranks are coloured in shared memory -- by a cluster of CTAs
+    (two by default, one or four here) with a copy of the colours in each --
+    and the rest by the grid-wide pull; where the boundary lies (1, 7, 64
+    ranks, or the default of 8192) and how many CTAs colour the core change no
+    colour.  A 2100-clique
+    (every vertex a long row inside the default core) forces colours past the
+    first 2048-colour window there."""
+    old = ecl.set_tune(gc_core_ranks=core, gc_core_ctas=ctas)
     try:
         cases = list(sym_cases(ecl)) + [("rmat16", ecl.gen_rmat(16, 16, seed=3))]
         if core == 0:
             cases.append(("clique2100", undirected(2100, [(i, j) for i in range(2100) for j in range(i + 1, 2100)])))
         for name, g in cases:
-            assert np.array_equal(ecl.gc(g), orc.gc(g)), (core, name)
+            assert np.array_equal(ecl.gc(g), orc.gc(g)), (core, ctas, name)
     finally:
         ecl.set_tune(old)
 
@@ -277,8 +280,8 @@ def test_cc_validate_checks_the_symmetric_flag(ecl):
 
 @pytest.mark.parametrize("knobs", [dict(row_lane_max=1, row_chunk=128), dict(row_lane_max=8, row_chunk=512),
                                    dict(row_lane_max=32, row_chunk=8192, blocks_per_sm=2),
-                                   dict(mst_light_factor=0.4, gc_core_ranks=5, gc_pull_blocks=4),
-                                   dict(gc_poll_ns=2048, row_vec=1, scc_sweep_batch=4, gc_pull_blocks=1)])
+                                   dict(mst_light_factor=0.4, gc_core_ranks=5, gc_pull_blocks=4, gc_core_ctas=4),
+                                   dict(gc_poll_ns=2048, row_vec=1, scc_sweep_batch=4, gc_pull_blocks=1, gc_core_ctas=2)])
 def test_launch_knobs_never_change_results(ecl, orc, knobs):
     """Every code under non-default degree bins, grid sizes, MST split and GC
     core size gives the oracle's result (hub rows cross every chunk size)."""
