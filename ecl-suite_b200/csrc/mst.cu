@@ -193,16 +193,26 @@ __device__ __forceinline__ void mst_emit_batch(int j0, int stride, int jend, boo
     const int j = j0 + k * stride;
     u[k] = (active && j < jend) ? __ldg(&nlist[j]) : -1;
   }
+  if (kLight) {
 #pragma unroll
-  for (int k = 0; k < kScanBatch; k++) {
-    const int j = j0 + k * stride;
-    w[k] = ((unsigned)u[k] < (unsigned)n && u[k] > v) ? __ldg(&eweight[j]) : 0;
-  }
+    for (int k = 0; k < kScanBatch; k++) {
+      const int j = j0 + k * stride;
+      w[k] = ((unsigned)u[k] < (unsigned)n && u[k] > v) ? __ldg(&eweight[j]) : 0;
+      ru[k] = -1;
+    }
+  } else {
+    // Heavy pass: the root first (flat after mst_flatten), the weight only
+    // for entries between two components.  The light pass joined the ends of
+    // every light entry (and checked every weight), so those are all heavy,
+    // and the ~80 % of entries inside one component cost no weight load.
 #pragma unroll
-  for (int k = 0; k < kScanBatch; k++) {
-    ru[k] = (!kLight && (unsigned)u[k] < (unsigned)n && u[k] > v && mst_keep<false>(w[k], thr))
-                ? ld(&parent[u[k]])  // flat after mst_flatten
-                : -1;
+    for (int k = 0; k < kScanBatch; k++)
+      ru[k] = ((unsigned)u[k] < (unsigned)n && u[k] > v) ? ld(&parent[u[k]]) : -1;
+#pragma unroll
+    for (int k = 0; k < kScanBatch; k++) {
+      const int j = j0 + k * stride;
+      w[k] = (ru[k] >= 0 && ru[k] != rv) ? __ldg(&eweight[j]) : 0;
+    }
   }
 #pragma unroll
   for (int k = 0; k < kScanBatch; k++) {
@@ -215,14 +225,14 @@ __device__ __forceinline__ void mst_emit_batch(int j0, int stride, int jend, boo
       } else if (u[k] > v) {
         if (w[k] < 0) {
           raise(status, ECL_ERR_BAD_GRAPH, j);
-        } else if (mst_keep<kLight>(w[k], thr)) {
-          if (kLight) {
+        } else if (kLight) {
+          if (mst_keep<true>(w[k], thr)) {
             keep = true;
             e = make_int4(v, u[k], w[k], j);
-          } else {
-            keep = ru[k] != rv;
-            e = make_int4(rv, ru[k], w[k], j);
           }
+        } else if (ru[k] != rv) {
+          keep = true;
+          e = make_int4(rv, ru[k], w[k], j);
         }
       }
     }
