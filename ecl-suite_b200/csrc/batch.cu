@@ -426,7 +426,7 @@ ecl_status ecl_batch_tune(ecl_batch* b, int32_t trials, ecl_tune* best) {
     void (*set)(ecl_tune&, float);
   };
   const std::vector<Knob> knobs = {
-      {true, {8.f, 4.f, 6.f}, [](ecl_tune& t, float v) { t.blocks_per_sm = (int32_t)v; }},
+      {true, {64.f, 32.f, 16.f, 8.f}, [](ecl_tune& t, float v) { t.blocks_per_sm = (int32_t)v; }},
       {(b->codes & ECL_BATCH_MST) != 0, {0.75f, 1.5f, 3.f, 0.4f}, [](ecl_tune& t, float v) { t.mst_light_factor = v; }},
       {true, {32.f, 16.f, 8.f}, [](ecl_tune& t, float v) { t.row_lane_max = (int32_t)v; }},
       {true, {256.f, 128.f, 512.f, 2048.f}, [](ecl_tune& t, float v) { t.row_chunk = (int32_t)v; }},

@@ -20,7 +20,7 @@ ecl_tune g_tune{};  // process-wide knobs of the single-graph entry points (unde
 bool tune_valid(const ecl_tune& t) {
   const bool chunk_ok = t.row_chunk == 0 || (t.row_chunk >= dev::kMinChunk && t.row_chunk <= dev::kMaxChunk &&
                                               (t.row_chunk & (t.row_chunk - 1)) == 0);
-  return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 8 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
+  return t.blocks_per_sm >= 0 && t.blocks_per_sm <= 128 && t.mst_light_factor >= 0.f && t.mst_light_factor <= 64.f &&
          t.gc_core_ranks >= 0 && t.gc_core_ranks <= 36864 && t.row_lane_max >= 0 && t.row_lane_max <= 32 && chunk_ok &&
          (t.scc_sweep_batch == 0 || t.scc_sweep_batch == 1 || t.scc_sweep_batch == 2 || t.scc_sweep_batch == 4) &&
          t.gc_poll_ns >= 0 && t.gc_poll_ns <= 4096 && (t.row_vec == 0 || t.row_vec == 1) &&

@@ -87,7 +87,7 @@ typedef struct ecl_opts {
  * (ECL-GC-atomic.cu:60-64,93), MST's warp path and light-edge sample
  * (ECL-MST_10-atomic.cu:197,450-459). */
 typedef struct ecl_tune {
-  int32_t blocks_per_sm;  /* blocks of 256 threads per SM for the grid-stride kernels; 0 = fill the SM */
+  int32_t blocks_per_sm;  /* blocks of 256 threads per SM in the grid-stride kernels' grids, 1..128; 0 = 64 */
   float mst_light_factor; /* MST light-edge target, in multiples of n; 0 = 0.75 */
   int32_t gc_core_ranks;  /* GC: leading ranks coloured in shared memory (the core), 0..36864; 0 = 8192 */
   int32_t row_lane_max;   /* CSR scans: rows of at most this many entries go to one lane, 0..32; 0 = per code */

@@ -39,7 +39,7 @@ def test_batch_tune_keeps_results(ecl, orc):
     b.build(ecl.BATCH_CC | ecl.BATCH_MIS | ecl.BATCH_MST)
     t = b.tune(trials=1)
     assert b.tune_points > 6
-    assert t.blocks_per_sm in (4, 6, 8) and t.mst_light_factor in (0.75, 1.5, 3.0, 0.4)
+    assert t.blocks_per_sm in (64, 32, 16, 8) and t.mst_light_factor in (0.75, 1.5, 3.0, 0.4)
     assert t.row_lane_max in (8, 16, 32) and t.row_chunk in (128, 256, 512, 2048)
     b.run()
     for i in range(b.graphs):
