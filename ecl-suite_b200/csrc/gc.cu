@@ -408,18 +408,20 @@ __device__ int gc_short_row(int beg, int h, const int* nl2, const int* color, St
 // On R-MAT the longest priority chain (about 2700 vertices at scale 22)
 // runs almost entirely through the long rows at the front of the order:
 // about 2200 of its hops lie in the first 16k ranks and 2470 in the first 32k.
-// A hop through L2 costs a store, a poll and a wake-up (about 1.7 us); in one
-// CTA's shared memory it costs a few hundred cycles.  So the first `core`
-// ranks (core = min(long rows, cap)) are coloured by ONE CTA of 32 warps with
-// their colours in shared memory, indexed by rank: every higher-priority
-// entry of a core row is itself a core vertex (it has a smaller rank), so a
-// core row never waits on global memory.  Two small launches first rewrite
+// A hop through L2 costs a store, a poll and a wake-up (about 1.5 us as the
+// pull achieves it); in shared memory it costs a few hundred cycles.  So the
+// first `core` ranks (core = min(long rows, cap)) are coloured by a cluster
+// of CTAs of 32 warps each (two by default) with the colours in shared
+// memory, indexed by rank -- a copy in every CTA, each colour stored into all
+// copies through distributed shared memory: every higher-priority entry of a
+// core row is itself a core vertex (it has a smaller rank), so a core row
+// never waits on global memory.  Two small launches first rewrite
 // the core rows' entries in nl2 from vertex ids to ranks (rank[] is the
 // inverse of the order over the core) and record each core rank's row
 // (start, length, vertex).
 //
-// One SM has to stream all core rows (16.6 M entries for the first 32k ranks
-// of R-MAT-22), and a warp that fetched each row with its own loads paid a
+// The cluster's SMs stream all core rows (16.6 M entries for the first 32k
+// ranks of R-MAT-22), and a warp that fetched each row with its own loads paid a
 // dependent L2 round trip per 128 entries.  Instead every warp stages its
 // rows through two shared-memory buffers with bulk asynchronous copies
 // (cp.async.bulk, completion counted on an mbarrier): while it colours one
