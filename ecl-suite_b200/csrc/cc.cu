@@ -448,7 +448,7 @@ ecl_status cc_enqueue(const GraphDev& g, int* parent, char* ws, Status* status, 
   int2* chunks;
   unsigned char* ing;
   cc_layout(c, g.n, g.m, &ctr, &chunks, &ing);
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, g.n, g.m);
   const Bins bins = bins_of(dev, kCCBins);
   const int cap = chunk_capacity(g.m, kMinChunk);  // cc_layout sized the records for the smallest chunk
   ECL_CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(CCCounters), stream));
@@ -609,7 +609,7 @@ extern "C" ecl_status ecl_cc_noalloc(int32_t nodes, int32_t edges, const int32_t
   // The array keeps the previous call's contents: clear the status block and
   // the counters (adjacent, at the front of the array) before every solve.
   ECL_CUDA_TRY(cudaMemsetAsync(base, 0, kStatusBytes + sizeof(CCCounters), stream));
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, nodes, edges);
   ECL_LAUNCH(cc_init<true>, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, status);
   ECL_LAUNCH(cc_hook, grid, kTPB, 0, stream, nodes, edges, nindex, nlist, label, chunks,
              chunk_capacity(edges, kCCBins.chunk), kCCBins, ctr, status);

@@ -953,7 +953,7 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gc_pull, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * std::min(occ, pull_blocks);
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, g.n, g.m);
   const RowChunks rc{b.chunks, &b.ctl->nchunks, (int)row_chunk_capacity(g.m, kMinChunk)};
   const Bins bins = bins_of(dev, Bins{kBinLane, kBinChunk});
   // key bits that vary: 32 hash bits + enough bits for any degree <= m

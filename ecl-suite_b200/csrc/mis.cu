@@ -289,7 +289,7 @@ ecl_status mis_enqueue(const GraphDev& g, unsigned char* out, char* ws, Status* 
   unsigned* st4;
   mis_layout(c, g.n, &st4);
   const int nwords = (g.n + 3) / 4;
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, g.n, g.m);
   const int* vbase = uni ? uni->vbase : nullptr;
   const float* avgs = uni ? uni->avg : nullptr;
   const int ngraphs = uni ? uni->ngraphs : 0;

@@ -722,7 +722,7 @@ ecl_status mst_enqueue(const GraphDev& g, unsigned char* in_mst, char* ws, Statu
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mst_boruvka, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, g.n, g.m);
   const Bins bins = bins_of(dev, kMstBins);
   // 16-byte row loads need 16-byte-aligned arrays (entries j = 0 mod 4 then are)
   const bool vec =

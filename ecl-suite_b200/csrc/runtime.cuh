@@ -3,6 +3,8 @@
 // the read-back of the device status word.
 #pragma once
 
+#include <algorithm>
+
 #include <cuda_runtime.h>
 
 #include <atomic>
@@ -109,9 +111,14 @@ struct DeviceInfo {
   // with more, smaller blocks the groups are dealt finer and the SMs that
   // finish early take new blocks: at R-MAT-22 the CSR scans ran 15-27 %
   // faster with 64 blocks per SM than with 8 (the suite 11.4 -> 10.6 ms).
-  int grid_blocks(int tpb) const {
+  // A small graph gets no more blocks than it has work for -- a thread per
+  // vertex, or per 8 CSR entries -- so concurrent solves of small graphs (the
+  // request server) do not queue behind thousands of empty blocks.
+  int grid_blocks(int tpb, long long n, long long m) const {
     const int per = blocks_per_sm > 0 ? blocks_per_sm : kGridBlocksPerSm;
-    return sms * (per * 256 / tpb > 0 ? per * 256 / tpb : 1);
+    const long long full = (long long)sms * (per * 256 / tpb > 0 ? per * 256 / tpb : 1);
+    const long long work = (std::max(n, m / 8) + tpb - 1) / tpb;
+    return (int)std::max(1LL, std::min(full, work));
   }
 };
 // Properties of the current device (cached per device id), with the

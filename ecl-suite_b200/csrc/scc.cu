@@ -417,7 +417,7 @@ ecl_status scc_enqueue(const GraphDev& g, int* label, char* ws, Status* status, 
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve, kTPB, 0) != cudaSuccess || occ < 1)
     return ECL_ERR_CUDA;
   const int coop_grid = dev.sms * occ;
-  const int grid = dev.grid_blocks(kTPB);
+  const int grid = dev.grid_blocks(kTPB, g.n, g.m);
   if (max_rounds <= 0 || max_rounds > b.max_rounds) max_rounds = b.max_rounds;
 
   if (cudaMemsetAsync(b.ctl, 0, sizeof(SCCCtl), stream) != cudaSuccess) return ECL_ERR_CUDA;
