@@ -575,28 +575,21 @@ __global__ void __launch_bounds__(kTPB) mst_boruvka(int n, int pass, int4* __res
       const int4 e = nx;
       const long long i1 = (long long)i + nthreads;
       nx = i1 < sz ? __ldcs(&in[i1]) : make_int4(-1, -1, 0, 0);
-      // one find per distinct endpoint per warp (the lanes holding it share
-      // the result)
-      const unsigned gx = __match_any_sync(kFull, e.x), gy = __match_any_sync(kFull, e.y);
-      const int lx = __ffs(gx) - 1, ly = __ffs(gy) - 1;
+      // each lane finds its own entry's roots (a per-lane memo, and the
+      // block's table ends a find at a known root without a load): grouping
+      // equal endpoints per warp first measured slower
       int ra = e.x, rb = e.y;  // round 0: the scan's entries hold roots
-      if (r > 0) {
-        if (valid && lane == lx) {
-          if (fx.key != e.x) {
-            fx.key = e.x;
-            fx.val = (u64)mst_find_a(e.x, parent, tab);
-          }
-          ra = (int)fx.val;
+      if (r > 0 && valid) {
+        if (fx.key != e.x) {
+          fx.key = e.x;
+          fx.val = (u64)mst_find_a(e.x, parent, tab);
         }
-        if (valid && lane == ly) {
-          if (fy.key != e.y) {
-            fy.key = e.y;
-            fy.val = (u64)mst_find_a(e.y, parent, tab);
-          }
-          rb = (int)fy.val;
+        ra = (int)fx.val;
+        if (fy.key != e.y) {
+          fy.key = e.y;
+          fy.val = (u64)mst_find_a(e.y, parent, tab);
         }
-        ra = __shfl_sync(kFull, ra, lx);
-        rb = __shfl_sync(kFull, rb, ly);
+        rb = (int)fy.val;
       }
       const bool keep = valid && ra != rb;
       if (r > 0) stg.push(keep, make_int4(ra, rb, e.z, e.w), out, &cnt[r + 1], cap, overflow);
