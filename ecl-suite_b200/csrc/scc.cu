@@ -68,7 +68,6 @@ __device__ __forceinline__ unsigned long long scc_now() {
   return t;
 }
 
-
 // In-max (high half) and out-max (low half) of one vertex.
 __device__ __forceinline__ unsigned long long io_pack(int in, int out) {
   return ((unsigned long long)(unsigned)in << 32) | (unsigned)out;
@@ -320,7 +319,7 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
         st(&ctl->changed[sweep], 1);
       }
       if (!grid_sync(&ctl->bar, status)) return;
-  if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
+      if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
       const bool again = ld(&ctl->changed[sweep]) != 0;
       sweep++;
       if (!again) {
@@ -360,7 +359,7 @@ __global__ void __launch_bounds__(kTPB, SweepOcc<kSweepBatch>::blocks) scc_solve
     }
     if (__any_sync(kFull, again) && lane == 0) st(&ctl->again[sweep - 1], 1);
     if (!grid_sync(&ctl->bar, status)) return;
-  if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
+    if (tid == 0 && ++nstamp < kStamps) ctl->stamp[nstamp] = scc_now();
     if (!ld(&ctl->again[sweep - 1])) break;
     size = min(ld(&ctl->kept[sweep - 1]), m0);
     int2* t = cur;
