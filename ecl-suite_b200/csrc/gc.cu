@@ -9,13 +9,14 @@
 //
 // B200 design: greedy colouring pulled in priority order.
 //  * gc_keys writes every vertex's priority key (the inverted (degree, hash)
-//    word); gc_init / gc_init_chunks (degree-binned: lane / warp / 256-entry
-//    chunk records) compare each list entry with one 8-byte key load and
-//    compact every row's higher-priority entries to the front of the row's
-//    slot in nl2[]; hc[v] = their number.
-//  * radix_sort_pairs then ranks all vertices by priority (a stable LSD sort
-//    of those keys over ids in descending order), which is a topological
-//    order of the colouring dependencies.
+//    word) and colours the isolated vertices 0; gc_init / gc_init_chunks
+//    (degree-binned: lane / warp / 256-entry chunk records) compare each
+//    list entry with one 8-byte key load and compact every row's
+//    higher-priority entries to the front of the row's slot in nl2[];
+//    hc[v] = their number.
+//  * radix_sort_pairs then ranks the vertices that have entries by priority
+//    (an LSD sort of their keys), which is a topological order of the
+//    colouring dependencies.
 //  * gc_pull is ONE cooperative persistent launch.  Ranks are dealt to the
 //    warps round-robin -- one long row (> 32 entries; they form a prefix of
 //    the order, priority being degree-first) or 32 short rows at a time --
@@ -54,7 +55,8 @@ constexpr int kWarpRow = 32;  // rows longer than this are coloured by a whole w
 struct GCCtl {
   int nchunks;
   int nbig;        // rows longer than kWarpRow: a prefix of the priority order
-  int pad2[30];
+  int nkeys;       // vertices with at least one entry: the ones sorted and pulled
+  int pad2[29];
 };
 
 // Priority hash of vertex x: the reference hashes the vertex id; in a union
@@ -201,12 +203,19 @@ __global__ void __launch_bounds__(kTPB) gc_init_chunks(int n, int m, const int* 
   }
 }
 
-// Sort keys: ascending order of ~((degree << 32) | hash) is descending
-// (degree, hash); the values start in descending id order, so the stable
-// sort breaks the remaining ties by descending id -- exactly the priority.
+// Priority keys: keys[n - 1 - v] = ~((degree << 32) | hash) for every v, the
+// array gc_init compares neighbours by; ascending order of the keys is
+// descending (degree, hash), the priority (within one graph the hash is a
+// bijection of the id, so no two vertices tie).  The vertices with at least
+// one entry are also appended to (skeys, svals), the sort's input, counted in
+// ctl->nkeys.  An isolated vertex has no neighbour to wait for or to block:
+// its colour is 0, written here, and it is neither sorted nor pulled
+// (R-MAT-22 has 1.8 M of them among its 4.2 M vertices).
 __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ nindex,
-                                                unsigned long long* __restrict__ keys, int* __restrict__ vals,
-                                                const unsigned* __restrict__ vhash, GCCtl* __restrict__ ctl) {
+                                                unsigned long long* __restrict__ keys,
+                                                unsigned long long* __restrict__ skeys, int* __restrict__ svals,
+                                                const unsigned* __restrict__ vhash, int* __restrict__ color,
+                                                GCCtl* __restrict__ ctl) {
   // rows longer than kWarpRow are counted per block and added once per block
   __shared__ int s_big;
   if (threadIdx.x == 0) s_big = 0;
@@ -214,15 +223,24 @@ __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ n
   int nb = 0;
   for (int base = (blockIdx.x * kTPB + threadIdx.x) & ~31; base < n; base += gridDim.x * kTPB) {
     const int i = base + (threadIdx.x & 31);
-    bool big = false;
+    bool big = false, linked = false;
+    unsigned long long key = 0;
+    int v = 0;
     if (i < n) {
-      const int v = n - 1 - i;
+      v = n - 1 - i;
       const unsigned deg = (unsigned)(__ldg(&nindex[v + 1]) - __ldg(&nindex[v]));
-      keys[i] = ~(((unsigned long long)deg << 32) | gc_h(vhash, v));
-      vals[i] = v;
+      key = ~(((unsigned long long)deg << 32) | gc_h(vhash, v));
+      keys[i] = key;
       big = deg > (unsigned)kWarpRow;
+      linked = deg > 0;
+      if (!linked) color[v] = 0;  // race-free: the output, thread-owned; nothing reads it in this launch
     }
     nb += __popc(__ballot_sync(kFull, big));
+    const int at = warp_append(&ctl->nkeys, linked);
+    if (linked) {
+      skeys[at] = key;
+      svals[at] = v;
+    }
   }
   if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&s_big, nb);
   __syncthreads();
@@ -886,10 +904,13 @@ __global__ void __launch_bounds__(kTPB) gc_pull(int n, const int* __restrict__ n
     if (lane == 0) st(&color[wv], c);
     __syncwarp();
   }
-  // Short rows: 32 consecutive ranks per warp step, every lane its own vertex.
-  for (int base = nbig + gwarp * 32; base < n; base += nwarps * 32) {
+  // Short rows: 32 consecutive ranks per warp step, every lane its own vertex
+  // (the order holds the nkeys vertices with entries; the isolated ones were
+  // coloured by gc_keys).
+  const int nk = min(ld(&ctl->nkeys), n);
+  for (int base = nbig + gwarp * 32; base < nk; base += nwarps * 32) {
     const int r = base + lane;
-    if (r < n) {
+    if (r < nk) {
       const int v = __ldg(&order[r]);
       const int c = gc_short_row(__ldg(&nindex[v]), __ldg(&hc[v]), nl2, color, status);
       if (c >= 0) st(&color[v], c);
@@ -968,14 +989,17 @@ ecl_status gc_enqueue(const GraphDev& g, int* color, char* ws, Status* status, c
     vhash = b.vhash;
   }
   // the priority keys first: gc_init compares neighbours by them
-  ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.vals0, vhash, b.ctl);
+  ECL_LAUNCH(gc_keys, grid, kTPB, 0, stream, g.n, g.nindex, b.keys0, b.keys1, b.vals1, vhash, color, b.ctl);
   const bool vec = (reinterpret_cast<uintptr_t>(g.nlist) & 15) == 0 && dev.row_vec;  // 16-byte row loads
   ECL_LAUNCH(gc_init, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins, vec, b.keys0, status);
   ECL_LAUNCH(gc_init_chunks, grid, kTPB, 0, stream, g.n, g.m, g.nindex, g.nlist, b.nl2, b.hc, rc, bins.chunk, vec, b.keys0,
              status);
   mark();
-  const bool in1 = radix_sort_pairs(b.keys0, b.vals0, b.keys1, b.vals1, g.n, 0, 32 + degbits, b.sort_temp, stream);
-  const int* order = in1 ? b.vals1 : b.vals0;
+  // the nkeys appended pairs, sorted from (keys1, vals1); the per-vertex keys
+  // in keys0 are dead once gc_init has run
+  const bool in0 = radix_sort_pairs(b.keys1, b.vals1, b.keys0, b.vals0, g.n, 0, 32 + degbits, b.sort_temp, stream,
+                                    &b.ctl->nkeys);
+  const int* order = in0 ? b.vals0 : b.vals1;
   mark();
   // the hub core (the sort keys are dead now: their buffer holds the ranks)
   const int cap = std::min(std::min(dev.gc_core_ranks > 0 ? dev.gc_core_ranks : kCoreDefault, kCoreMax), g.n);
