@@ -216,13 +216,17 @@ __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ n
                                                 unsigned long long* __restrict__ skeys, int* __restrict__ svals,
                                                 const unsigned* __restrict__ vhash, int* __restrict__ color,
                                                 GCCtl* __restrict__ ctl) {
-  // rows longer than kWarpRow are counted per block and added once per block
+  // rows longer than kWarpRow are counted per block and added once per block;
+  // the appends reserve their room with one atomic per block and step
   __shared__ int s_big;
+  __shared__ int s_woff[kTPB / 32];
+  __shared__ int s_base;
   if (threadIdx.x == 0) s_big = 0;
   __syncthreads();
   int nb = 0;
-  for (int base = (blockIdx.x * kTPB + threadIdx.x) & ~31; base < n; base += gridDim.x * kTPB) {
-    const int i = base + (threadIdx.x & 31);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int bbase = blockIdx.x * kTPB; bbase < n; bbase += gridDim.x * kTPB) {  // block-uniform trip count
+    const int i = bbase + threadIdx.x;
     bool big = false, linked = false;
     unsigned long long key = 0;
     int v = 0;
@@ -236,11 +240,25 @@ __global__ void __launch_bounds__(kTPB) gc_keys(int n, const int* __restrict__ n
       if (!linked) color[v] = 0;  // race-free: the output, thread-owned; nothing reads it in this launch
     }
     nb += __popc(__ballot_sync(kFull, big));
-    const int at = warp_append(&ctl->nkeys, linked);
+    const unsigned bal = __ballot_sync(kFull, linked);
+    if (lane == 0) s_woff[wid] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int run = 0;
+      for (int w = 0; w < kTPB / 32; w++) {
+        const int c = s_woff[w];
+        s_woff[w] = run;
+        run += c;
+      }
+      s_base = run ? fetch_add(&ctl->nkeys, run) : 0;
+    }
+    __syncthreads();
     if (linked) {
+      const int at = s_base + s_woff[wid] + __popc(bal & ((1u << lane) - 1));
       skeys[at] = key;
       svals[at] = v;
     }
+    __syncthreads();  // s_woff and s_base are rewritten next step
   }
   if ((threadIdx.x & 31) == 0 && nb) atomicAdd(&s_big, nb);
   __syncthreads();
